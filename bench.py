@@ -1,0 +1,315 @@
+"""Benchmark of the FP64 FR residual (rhs_func) on the large blast workload.
+
+Workload: 2D radial blast on [0,1]^2, 1024 x 1024 quads, GLL p = 5 (36 points per
+element), HLLC, Van der Waals gas (a = 0.05, b = 0.02, gamma = 1.4): 37,748,736
+nodes, 150,994,944 DOF, a 1.21 GB FP64 state (larger than the 126 MB L2, so no
+flush is needed between steps).  One step = one rhs = -R(U) over the whole mesh.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one process per GPU, each rank on its own replica of
+the workload (weak scaling); rank 0 prints one JSON line.  --impl reference
+times the CPU restatement of the reference's residual (oracle/) on the host
+cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "DOF-residuals/s (FP64 FR residual, rhs_func)"
+UNIT = "DOF-residuals/s"
+WORKLOAD = "blast_vdw_1024x1024_p5 (2D radial blast, HLLC, Van der Waals a=0.05 b=0.02, filter + shock sensor)"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_launch():
+    """DRAM bytes per launch of the residual kernel from the committed ncu summary."""
+    f = ROOT / "profiles" / "fr2d_kernel_blast_traffic.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("dram_bytes_per_full_launch:"):
+            return float(line.split(":", 1)[1].strip())
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_residual_rate(threads: int, target_s: float = 3.0, rows: int = 64, max_reps: int = 20):
+    """Oracle (CPU restatement) residual rate on a bounded sample of the workload:
+    a 1024 x `rows` element strip of the same mesh spacing and state."""
+    import numpy as np
+
+    from fr_sdg_b200.workloads import blast_large
+    from oracle.oracle import Oracle
+
+    wl = blast_large()
+    cfg = wl.cfg
+    full = wl.init("cpu").numpy()
+    n = cfg.poly_deg + 1
+    per_row = cfg.n_elems[0] * n * n * 4
+    j0 = cfg.n_elems[1] // 2 - rows // 2
+    U = np.ascontiguousarray(full[j0 * per_row:(j0 + rows) * per_row])
+    del full
+    cfg.n_elems[1] = rows
+    cfg.box_length[1] = rows / 1024.0
+    o = Oracle(cfg, threads=threads)
+    o.residual(0.0, U)  # warm
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        o.residual(0.0, U)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= target_s or reps >= max_reps:
+            break
+    dofs = U.size
+    return dofs * reps / el, {"sample": f"{reps} residual(s) of a 1024x{rows}-element strip of the workload "
+                                        f"({dofs} DOF each), {el:.1f} s wall",
+                              "cores": threads}
+
+
+def run_reference(args, ws, rank):
+    """--impl reference: the CPU restatement of the reference residual on all host cores."""
+    if rank != 0:
+        return 0
+    from oracle import oracle
+
+    oracle.lib()
+    threads = os.cpu_count() or 1
+    rates = []
+    for _ in range(args.warmup):
+        cpu_residual_rate(threads, target_s=0.0, max_reps=1)
+    for _ in range(args.steps):
+        r, info = cpu_residual_rate(threads, target_s=0.0, max_reps=1)
+        rates.append(r)
+    value = statistics.median(rates)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "parallelism": "host threads (OpenMP over element rows)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": info["sample"] + " per step; the reference binary needs PETSc/MPI/Eigen/Boost "
+                                                    "and is not buildable here, so the oracle restatement runs"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+
+    from fr_sdg_b200 import FRSolver
+    from fr_sdg_b200.workloads import blast_large
+
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    wl = blast_large()
+    solver = FRSolver(wl.cfg)
+    U = wl.init(f"cuda:{local}")
+    F = torch.empty_like(U)
+    dofs = U.numel()
+    stream = torch.cuda.current_stream()
+
+    for _ in range(args.warmup):
+        solver.rhs_func(0.0, U, F)
+    torch.cuda.synchronize()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for k in range(args.steps):
+            starts[k].record(stream)
+            solver.rhs_func(0.0, U, F)
+            ends[k].record(stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    elapsed_ms = t0.elapsed_time(t1)
+    launch_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    if dist:
+        t = torch.tensor([elapsed_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    value = ws * dofs * args.steps / (elapsed_ms / 1e3)
+    bad = solver.status()
+
+    # ---- end to end through the host-buffer entry point
+    e2e = None
+    if not args.no_e2e:
+        Uh = U.cpu().pin_memory()
+        Fh = torch.empty_like(Uh).pin_memory()
+        solver.rhs_func_host(0.0, Uh, Fh)  # allocates the staging buffers once
+        ke = max(1, min(args.steps, args.e2e_steps))
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(ke):
+            solver.rhs_func_host(0.0, Uh, Fh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ems = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ems], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": ws * dofs * ke / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": Uh.numel() * 8,
+               "d2h_bytes_per_step": Fh.numel() * 8, "steps": ke,
+               "path": "frsdg_rhs_host (pinned host U -> device -> rhs -> pinned host)"}
+
+    # ---- roofline of the residual kernel
+    peak, peak_kind = measured_peaks()
+    alg_bytes = dofs * 8 * 2  # read U, write rhs (affine mesh: metrics are constants)
+    mean_launch_s = statistics.mean(launch_ms) / 1e3
+    achieved = alg_bytes / mean_launch_s / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic_per_launch(), "peak_kind": peak_kind, "kernel": "fr2d_kernel<double,6,VdW,HLLC,affine>",
+            "algorithmic_bytes_per_launch": alg_bytes, "mean_launch_ms": mean_launch_s * 1e3}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        from oracle import oracle
+
+        oracle.lib()
+        threads = os.cpu_count() or 1
+        r1, info1 = cpu_residual_rate(1, target_s=10.0, rows=16, max_reps=20)
+        cpu = {"value": r1, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": info1["sample"] + "; oracle restatement of the reference residual, 1 thread"}
+        if args.cpu_all_cores:
+            rN, infoN = cpu_residual_rate(threads, target_s=10.0, max_reps=20)
+            cpu["all_cores"] = {"value": rN, "cores": threads, "sample": infoN["sample"]}
+
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "elements": [1024, 1024], "poly_deg": 5, "dofs_per_rank": dofs,
+                   "state_bytes": dofs * 8, "l2": "inputs (1.21 GB) larger than L2 (126 MB); no flush",
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+        "clocks": clk.summary(), "gpu_launches": args.steps, "roofline": roof, "e2e": e2e,
+        "cpu_baseline": cpu, "bad_density_nodes": bad,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-all-cores", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, ws, rank)
+    return run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

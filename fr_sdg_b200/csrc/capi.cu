@@ -1,0 +1,620 @@
+// capi.cu -- implementation of the C ABI in include/frsdg.h.
+//
+// The handle plays the role of the reference's PhysicsEvaluator + PetscSolver pair
+// (physics_evaluator.hpp:158-318, petsc_solver_impl.hpp:444-755): it owns the
+// reference element, the filter, the cached curved metrics, the boundary data
+// and every workspace, and it turns each PETSc callback into one kernel launch.
+#include "../../include/frsdg.h"
+#include "device_math.cuh"
+#include "frsdg_internal.hpp"
+#include "setup_ops.hpp"
+#include "stab.hpp"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <string>
+#include <vector>
+
+using namespace frsdg;
+
+namespace frsdg
+{
+// explicit instantiations live in residual2d_n*.cu / residual1d.cu
+#define FRSDG_DECL(S, N)                                                                                       \
+    extern template cudaError_t launch_fr2d<S, N>(int, int, int, const Fr2dArgs&, cudaStream_t);              \
+    extern template cudaError_t launch_fr1d<S, N>(int, int, const Fr1dArgs&, cudaStream_t);
+#define FRSDG_DECL_ALL(S)                                                                                      \
+    FRSDG_DECL(S, 2) FRSDG_DECL(S, 3) FRSDG_DECL(S, 4) FRSDG_DECL(S, 5) FRSDG_DECL(S, 6) FRSDG_DECL(S, 7)    \
+    FRSDG_DECL(S, 8) FRSDG_DECL(S, 9) FRSDG_DECL(S, 10)
+FRSDG_DECL_ALL(double)
+FRSDG_DECL_ALL(cplx)
+} // namespace frsdg
+
+namespace
+{
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg)
+{
+    g_err = msg;
+    return code;
+}
+int cuda_fail(cudaError_t e, const char* what)
+{
+    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    return FRSDG_ERR_CUDA;
+}
+
+template <class S> cudaError_t dispatch2d(int n, int gas, int riem, int geo, const Fr2dArgs& a, cudaStream_t s)
+{
+    switch (n)
+    {
+        case 2: return launch_fr2d<S, 2>(gas, riem, geo, a, s);
+        case 3: return launch_fr2d<S, 3>(gas, riem, geo, a, s);
+        case 4: return launch_fr2d<S, 4>(gas, riem, geo, a, s);
+        case 5: return launch_fr2d<S, 5>(gas, riem, geo, a, s);
+        case 6: return launch_fr2d<S, 6>(gas, riem, geo, a, s);
+        case 7: return launch_fr2d<S, 7>(gas, riem, geo, a, s);
+        case 8: return launch_fr2d<S, 8>(gas, riem, geo, a, s);
+        case 9: return launch_fr2d<S, 9>(gas, riem, geo, a, s);
+        case 10: return launch_fr2d<S, 10>(gas, riem, geo, a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+template <class S> cudaError_t dispatch1d(int n, int gas, int riem, const Fr1dArgs& a, cudaStream_t s)
+{
+    switch (n)
+    {
+        case 2: return launch_fr1d<S, 2>(gas, riem, a, s);
+        case 3: return launch_fr1d<S, 3>(gas, riem, a, s);
+        case 4: return launch_fr1d<S, 4>(gas, riem, a, s);
+        case 5: return launch_fr1d<S, 5>(gas, riem, a, s);
+        case 6: return launch_fr1d<S, 6>(gas, riem, a, s);
+        case 7: return launch_fr1d<S, 7>(gas, riem, a, s);
+        case 8: return launch_fr1d<S, 8>(gas, riem, a, s);
+        case 9: return launch_fr1d<S, 9>(gas, riem, a, s);
+        case 10: return launch_fr1d<S, 10>(gas, riem, a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+bool is_native_bc(int k) { return k == FRSDG_BC_OUTFLOW || k == FRSDG_BC_WALL || k == FRSDG_BC_PERIODIC; }
+
+int validate(const frsdg_config& c)
+{
+    if (c.dim != 1 && c.dim != 2) return fail(FRSDG_ERR_ARG, "dim must be 1 or 2");
+    if (c.poly_deg < 1 || c.poly_deg > 9) return fail(FRSDG_ERR_ARG, "poly_deg must be in [1, 9]");
+    if (c.n_elems[0] < 2 || (c.dim == 2 && c.n_elems[1] < 2))
+        return fail(FRSDG_ERR_ARG, "n_elems must be >= 2 in every direction");
+    if (!(c.box_length[0] > 0.0) || (c.dim == 2 && !(c.box_length[1] > 0.0)))
+        return fail(FRSDG_ERR_ARG, "box_length must be positive");
+    if (c.gas_law != FRSDG_GAS_IDEAL && c.gas_law != FRSDG_GAS_VDW) return fail(FRSDG_ERR_ARG, "unknown gas_law");
+    if (c.riemann != FRSDG_RUSANOV && c.riemann != FRSDG_HLLC) return fail(FRSDG_ERR_ARG, "unknown riemann scheme");
+    if (!(c.gamma > 1.0)) return fail(FRSDG_ERR_ARG, "gamma must be > 1");
+    if (c.dim == 2 && (c.geometry < 0 || c.geometry > FRSDG_GEOM_SINE_WARP)) return fail(FRSDG_ERR_ARG, "unknown geometry");
+    if (c.coord_sys == FRSDG_COORD_RADIAL && c.dim != 1) return fail(FRSDG_ERR_UNSUPPORTED, "radial coordinates are 1D only");
+    const int nb = c.dim == 2 ? 4 : 2;
+    for (int d = 0; d < nb; ++d)
+        if (c.bc[d].kind < 0 || c.bc[d].kind > FRSDG_BC_PRESSURE_OUTLET) return fail(FRSDG_ERR_ARG, "unknown bc kind");
+    auto per = [&](int a, int b) { return c.bc[a].kind == FRSDG_BC_PERIODIC || c.bc[b].kind == FRSDG_BC_PERIODIC; };
+    auto both = [&](int a, int b) { return c.bc[a].kind == FRSDG_BC_PERIODIC && c.bc[b].kind == FRSDG_BC_PERIODIC; };
+    if (per(FRSDG_LEFT, FRSDG_RIGHT) && !both(FRSDG_LEFT, FRSDG_RIGHT))
+        return fail(FRSDG_ERR_ARG, "periodic x needs both LEFT and RIGHT periodic");
+    if (c.dim == 2 && per(FRSDG_TOP, FRSDG_BOTTOM) && !both(FRSDG_TOP, FRSDG_BOTTOM))
+        return fail(FRSDG_ERR_ARG, "periodic y needs both TOP and BOTTOM periodic");
+    if (c.dim == 1)
+        for (int d = 0; d < 2; ++d)
+            if (c.bc[d].kind > FRSDG_BC_DIRICHLET) return fail(FRSDG_ERR_UNSUPPORTED, "1D supports outflow, wall, periodic, dirichlet");
+    if (c.apply_filter && c.filt_cut_off == c.poly_deg)
+        return fail(FRSDG_ERR_ARG, "filter cut-off equal to poly_deg gives 0/0 in the filter strength");
+    if (c.apply_weno && (c.weno_gamma > 1.0 || c.weno_gamma < 0.0)) return fail(FRSDG_ERR_ARG, "weno_gamma must be in [0,1]");
+    if (!(c.csd_eps > 0.0)) return fail(FRSDG_ERR_ARG, "csd_eps must be positive");
+    return FRSDG_OK;
+}
+
+} // namespace
+
+struct frsdg_handle
+{
+    frsdg_config cfg{};
+    int          n = 0, Nx = 0, Ny = 0, ndofs = 0;
+    int64_t      ntot = 0, nelem = 0;
+    int          geo = GEO_AFFINE;
+    RefElem      re;
+    Fr2dArgs     a2{};   // template of the 2D launch arguments
+    Fr1dArgs     a1{};
+    StabArgs     st{};
+    double*      d_metrics = nullptr;
+    double*      d_xnorm = nullptr;
+    double*      d_ynorm = nullptr;
+    double*      d_bxy = nullptr;
+    double*      d_work = nullptr;   // post-step source copy (WENO)
+    double*      d_stage = nullptr;  // host-buffer staging (2 * ntot), allocated on first use
+    unsigned long long* d_bad = nullptr;
+    double       jvp_t = 0.0, jvp_sigma = 1.0;
+    const double* jvp_U = nullptr;
+    cudaStream_t last = nullptr;
+    int          device = 0;
+};
+
+static void free_handle(frsdg_handle* h)
+{
+    if (!h) return;
+    cudaFree(h->d_metrics);
+    cudaFree(h->d_xnorm);
+    cudaFree(h->d_ynorm);
+    cudaFree(h->d_bxy);
+    cudaFree(h->d_work);
+    cudaFree(h->d_stage);
+    cudaFree(h->d_bad);
+    delete h;
+}
+
+template <class T> static int upload(T** dst, const std::vector<T>& v)
+{
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(dst), sizeof(T) * (v.empty() ? 1 : v.size()));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+    if (!v.empty())
+    {
+        e = cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy");
+    }
+    return FRSDG_OK;
+}
+
+extern "C" {
+
+int frsdg_abi_version(void) { return FRSDG_ABI_VERSION; }
+const char* frsdg_last_error(void) { return g_err.c_str(); }
+
+int frsdg_config_default(frsdg_config* c)
+{
+    if (!c) return fail(FRSDG_ERR_ARG, "null config");
+    std::memset(c, 0, sizeof(*c));
+    c->dim = 2;
+    c->poly_deg = 3;
+    c->n_elems[0] = c->n_elems[1] = 10;
+    c->box_length[0] = c->box_length[1] = 1.0;
+    c->radau_corr = 0.0;
+    c->gas_law = FRSDG_GAS_IDEAL;
+    c->riemann = FRSDG_RUSANOV;
+    c->gamma = 1.4;
+    c->R_spec = 287.05;
+    c->vdw_a = 161.94;
+    c->vdw_b = 0.001265;
+    c->coord_sys = FRSDG_COORD_CARTESIAN;
+    c->geometry = FRSDG_GEOM_CARTESIAN;
+    c->geom_profile = FRSDG_PROFILE_FLAT;
+    for (int d = 0; d < 4; ++d) c->bc[d].kind = FRSDG_BC_OUTFLOW;
+    c->apply_filter = 0;
+    c->filt_cut_off = 2;
+    c->filt_strength = 32;
+    c->filt_alpha = 36.0;
+    c->apply_weno = 0;
+    c->weno_gamma = 0.998;
+    c->shock_theta = 1.0;
+    c->shock_threshold = 0.8;
+    c->cond_sys = 0;
+    c->csd_eps = 1e-7;
+    return FRSDG_OK;
+}
+
+int frsdg_reference_element(int32_t p, double c, double* nodes, double* w, double* D, double* dL, double* dR)
+{
+    try
+    {
+        const RefElem r = build_ref_element(p, c);
+        if (nodes) std::memcpy(nodes, r.x.data(), sizeof(double) * r.n);
+        if (w) std::memcpy(w, r.w.data(), sizeof(double) * r.n);
+        if (D) std::memcpy(D, r.D.data(), sizeof(double) * r.n * r.n);
+        if (dL) std::memcpy(dL, r.dL.data(), sizeof(double) * r.n);
+        if (dR) std::memcpy(dR, r.dR.data(), sizeof(double) * r.n);
+        return FRSDG_OK;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(FRSDG_ERR_ARG, e.what());
+    }
+}
+
+int frsdg_filter_matrix(int32_t p, int32_t cut_off, int32_t strength, double alpha, double* F)
+{
+    try
+    {
+        const RefElem r = build_ref_element(p, 0.0);
+        const auto    f = build_filter_matrix(r, cut_off, strength, alpha);
+        std::memcpy(F, f.data(), sizeof(double) * f.size());
+        return FRSDG_OK;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(FRSDG_ERR_ARG, e.what());
+    }
+}
+
+int frsdg_create(const frsdg_config* cfg, frsdg_handle** out)
+{
+    if (!cfg || !out) return fail(FRSDG_ERR_ARG, "null argument");
+    *out = nullptr;
+    int rc = validate(*cfg);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    {
+        cudaGetLastError();
+        return fail(FRSDG_ERR_NODEVICE, "no CUDA device visible");
+    }
+    auto* h = new frsdg_handle();
+    h->cfg = *cfg;
+    cudaGetDevice(&h->device);
+    try
+    {
+        h->re = build_ref_element(cfg->poly_deg, cfg->radau_corr);
+    }
+    catch (const std::exception& e)
+    {
+        delete h;
+        return fail(FRSDG_ERR_ARG, e.what());
+    }
+    const int n = h->re.n;
+    h->n = n;
+    h->Nx = cfg->n_elems[0];
+    h->Ny = cfg->dim == 2 ? cfg->n_elems[1] : 1;
+    h->ndofs = cfg->dim == 2 ? 4 * n * n : 3 * n;
+    h->nelem = int64_t(h->Nx) * h->Ny;
+    h->ntot = h->nelem * h->ndofs;
+
+    Ops ops{};
+    for (int q = 0; q < n * n; ++q) ops.D[q] = h->re.D[q];
+    for (int q = 0; q < n; ++q) { ops.dL[q] = h->re.dL[q]; ops.dR[q] = h->re.dR[q]; ops.csi[q] = h->re.x[q]; }
+    const GasParams gas{cfg->gamma, cfg->gas_law == FRSDG_GAS_VDW ? cfg->vdw_a : 0.0,
+                        cfg->gas_law == FRSDG_GAS_VDW ? cfg->vdw_b : 0.0};
+    const bool per_x = cfg->bc[FRSDG_LEFT].kind == FRSDG_BC_PERIODIC;
+    const bool per_y = cfg->dim == 2 && cfg->bc[FRSDG_TOP].kind == FRSDG_BC_PERIODIC;
+
+    if ((rc = upload(&h->d_bad, std::vector<unsigned long long>{0ull})))
+    {
+        free_handle(h);
+        return rc;
+    }
+
+    if (cfg->dim == 2)
+    {
+        const int Nx = h->Nx, Ny = h->Ny;
+        GeometryMap geom(*cfg);
+        const double hx = 1.0 / double(Nx), hy = 1.0 / double(Ny);
+        auto comp_x = [&](int i, int k) { return hx * (double(i) + 0.5 * (1.0 + h->re.x[k])); };
+        auto comp_y = [&](int j, int l) { return hy * (double(j) + 0.5 * (1.0 + h->re.x[l])); };
+        // composite metrics of physics_evaluator.hpp:282-305
+        auto metrics = [&](double cx, double cy, double m[4]) {
+            const GeomJacobian g = geom.jacobian(cx, cy);
+            const double dcsi_dr = 0.5 / double(Nx), deta_ds = 0.5 / double(Ny);
+            const double dx_dr = g.dx_dcsi * dcsi_dr, dy_dr = g.dy_dcsi * dcsi_dr;
+            const double dx_ds = g.dx_deta * deta_ds, dy_ds = g.dy_deta * deta_ds;
+            const double detJ = dx_dr * dy_ds - dx_ds * dy_dr;
+            m[0] = dy_ds / detJ;
+            m[1] = -dx_ds / detJ;
+            m[2] = -dy_dr / detJ;
+            m[3] = dx_dr / detJ;
+        };
+        Fr2dArgs& a = h->a2;
+        a.Nx = Nx;
+        a.Ny = Ny;
+        a.per_x = per_x;
+        a.per_y = per_y;
+        a.gas = gas;
+        a.Lx = cfg->box_length[0];
+        a.Ly = cfg->box_length[1];
+        a.ops = ops;
+        a.bad = h->d_bad;
+        for (int d = 0; d < 4; ++d)
+        {
+            a.bc[d].kind = cfg->bc[d].kind;
+            for (int q = 0; q < 4; ++q) a.bc[d].state[q] = cfg->bc[d].state[q];
+            for (int q = 0; q < 6; ++q) a.bc[d].params[q] = cfg->bc[d].params[q];
+        }
+        h->geo = geom.affine() ? GEO_AFFINE : GEO_CURVED;
+        {
+            double m[4];
+            metrics(0.5, 0.5, m);
+            a.xi_x = m[0]; a.xi_y = m[1]; a.eta_x = m[2]; a.eta_y = m[3];
+            a.scale_x = std::sqrt(m[0] * m[0] + m[1] * m[1]);
+            a.scale_y = std::sqrt(m[2] * m[2] + m[3] * m[3]);
+        }
+        try
+        {
+            if (h->geo == GEO_CURVED)
+            {
+                std::vector<double> mt(size_t(h->nelem) * n * n * 4);
+                for (int j = 0; j < Ny; ++j)
+                    for (int i = 0; i < Nx; ++i)
+                        for (int l = 0; l < n; ++l)
+                            for (int k = 0; k < n; ++k)
+                                metrics(comp_x(i, k), comp_y(j, l),
+                                        &mt[(((size_t(j) * Nx + i) * n + l) * n + k) * 4]);
+                std::vector<double> xn(size_t(Nx + 1) * Ny * n * 2), yn(size_t(Nx) * (Ny + 1) * n * 2);
+                for (int j = 0; j < Ny; ++j)
+                    for (int I = 0; I <= Nx; ++I)
+                        for (int l = 0; l < n; ++l)
+                        {
+                            const auto nn = geom.x_face_normal(comp_x(I, 0), comp_y(j, l));
+                            const size_t o = ((size_t(j) * (Nx + 1) + I) * n + l) * 2;
+                            xn[o] = nn.first;
+                            xn[o + 1] = nn.second;
+                        }
+                for (int J = 0; J <= Ny; ++J)
+                    for (int i = 0; i < Nx; ++i)
+                        for (int k = 0; k < n; ++k)
+                        {
+                            const auto nn = geom.y_face_normal(comp_x(i, k), comp_y(J, 0));
+                            const size_t o = ((size_t(J) * Nx + i) * n + k) * 2;
+                            yn[o] = nn.first;
+                            yn[o + 1] = nn.second;
+                        }
+                if ((rc = upload(&h->d_metrics, mt)) || (rc = upload(&h->d_xnorm, xn)) || (rc = upload(&h->d_ynorm, yn)))
+                {
+                    free_handle(h);
+                    return rc;
+                }
+            }
+            // boundary face points: LEFT, RIGHT (Ny*n each), TOP, BOTTOM (Nx*n each)
+            std::vector<double> bxy(size_t(2 * Ny * n + 2 * Nx * n) * 2);
+            size_t off[4];
+            off[FRSDG_LEFT] = 0;
+            off[FRSDG_RIGHT] = size_t(Ny) * n * 2;
+            off[FRSDG_TOP] = size_t(2 * Ny) * n * 2;
+            off[FRSDG_BOTTOM] = off[FRSDG_TOP] + size_t(Nx) * n * 2;
+            for (int j = 0; j < Ny; ++j)
+                for (int l = 0; l < n; ++l)
+                {
+                    const auto pl = geom.physical(comp_x(0, 0), comp_y(j, l));
+                    const auto pr = geom.physical(comp_x(Nx, 0), comp_y(j, l));
+                    bxy[off[FRSDG_LEFT] + (j * n + l) * 2] = pl.first;
+                    bxy[off[FRSDG_LEFT] + (j * n + l) * 2 + 1] = pl.second;
+                    bxy[off[FRSDG_RIGHT] + (j * n + l) * 2] = pr.first;
+                    bxy[off[FRSDG_RIGHT] + (j * n + l) * 2 + 1] = pr.second;
+                }
+            for (int i = 0; i < Nx; ++i)
+                for (int k = 0; k < n; ++k)
+                {
+                    const auto pb = geom.physical(comp_x(i, k), comp_y(0, 0));
+                    const auto pt = geom.physical(comp_x(i, k), comp_y(Ny, 0));
+                    bxy[off[FRSDG_BOTTOM] + (i * n + k) * 2] = pb.first;
+                    bxy[off[FRSDG_BOTTOM] + (i * n + k) * 2 + 1] = pb.second;
+                    bxy[off[FRSDG_TOP] + (i * n + k) * 2] = pt.first;
+                    bxy[off[FRSDG_TOP] + (i * n + k) * 2 + 1] = pt.second;
+                }
+            if ((rc = upload(&h->d_bxy, bxy)))
+            {
+                free_handle(h);
+                return rc;
+            }
+            for (int d = 0; d < 4; ++d) a.bxy[d] = h->d_bxy + off[d];
+        }
+        catch (const std::exception& e)
+        {
+            free_handle(h);
+            return fail(FRSDG_ERR_NOMEM, e.what());
+        }
+        a.metrics = h->d_metrics;
+        a.xnorm = h->d_xnorm;
+        a.ynorm = h->d_ynorm;
+    }
+    else
+    {
+        Fr1dArgs& a = h->a1;
+        a.N = h->Nx;
+        a.per = per_x;
+        a.gas = gas;
+        a.h_elem = cfg->box_length[0] / cfg->n_elems[0];
+        a.inv_jac = 2.0 / a.h_elem;
+        a.radial = cfg->coord_sys == FRSDG_COORD_RADIAL;
+        for (int d = 0; d < 2; ++d)
+        {
+            a.bc[d].kind = cfg->bc[d].kind;
+            for (int q = 0; q < 4; ++q) a.bc[d].state[q] = cfg->bc[d].state[q];
+        }
+        a.ops = ops;
+        a.bad = h->d_bad;
+    }
+
+    // post-step stabilisation
+    {
+        StabArgs& s = h->st;
+        s.dim = cfg->dim;
+        s.Nx = h->Nx;
+        s.Ny = h->Ny;
+        s.per_x = per_x;
+        s.per_y = per_y;
+        s.apply_filter = cfg->apply_filter;
+        s.apply_weno = cfg->apply_weno;
+        const double g = cfg->weno_gamma;
+        s.gam[0] = (1 - g) * 0.5;
+        s.gam[1] = g;
+        s.gam[2] = (1 - g) * 0.5;
+        const double dmin = std::fmin(s.gam[0], std::fmin(s.gam[1], s.gam[2]));
+        s.one_over_norm = 1.0 / (std::pow(std::fabs(1.0 / dmin - 1.0), cfg->shock_theta) + 3.0 - 1.0);
+        s.theta = cfg->shock_theta;
+        s.threshold = cfg->shock_threshold;
+        const auto F = build_filter_matrix(h->re, cfg->filt_cut_off, cfg->filt_strength, cfg->filt_alpha);
+        for (int q = 0; q < n * n; ++q) { s.F[q] = F[q]; s.D[q] = h->re.D[q]; }
+        for (int q = 0; q < n; ++q) s.w[q] = h->re.w[q];
+        if (cfg->apply_weno && !cfg->apply_filter)
+        {
+            cudaError_t e = cudaMalloc(&h->d_work, sizeof(double) * h->ntot);
+            if (e != cudaSuccess)
+            {
+                free_handle(h);
+                return cuda_fail(e, "cudaMalloc(post-step workspace)");
+            }
+        }
+    }
+    *out = h;
+    return FRSDG_OK;
+}
+
+int frsdg_destroy(frsdg_handle* h)
+{
+    free_handle(h);
+    return FRSDG_OK;
+}
+
+int frsdg_n_dofs(const frsdg_handle* h, int64_t* n)
+{
+    if (!h || !n) return fail(FRSDG_ERR_ARG, "null argument");
+    *n = h->ntot;
+    return FRSDG_OK;
+}
+
+} // extern "C"
+
+namespace
+{
+int run_residual(frsdg_handle* h, int mode, double t, const double* U, const double* W, double* out, void* stream)
+{
+    if (!h || !U || !out) return fail(FRSDG_ERR_ARG, "null argument");
+    if ((reinterpret_cast<uintptr_t>(U) | reinterpret_cast<uintptr_t>(out)) & 15)
+        return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    h->last = s;
+    const bool cvar = (mode == MODE_IFUNC || mode == MODE_JVP) && h->cfg.cond_sys;
+    const double hh = h->cfg.csd_eps;
+    cudaError_t e;
+    if (h->cfg.dim == 2)
+    {
+        Fr2dArgs a = h->a2;
+        a.t = t;
+        a.mode = mode;
+        a.cond_sys = cvar;
+        a.U = U;
+        a.W = W;
+        a.out = out;
+        a.h = hh;
+        a.inv_h = 1.0 / hh;
+        a.sigma = h->jvp_sigma;
+        if (mode == MODE_JVP) e = dispatch2d<cplx>(h->n, h->cfg.gas_law, h->cfg.riemann, h->geo, a, s);
+        else e = dispatch2d<double>(h->n, h->cfg.gas_law, h->cfg.riemann, h->geo, a, s);
+    }
+    else
+    {
+        Fr1dArgs a = h->a1;
+        a.t = t;
+        a.mode = mode;
+        a.cond_sys = cvar;
+        a.U = U;
+        a.W = W;
+        a.out = out;
+        a.h = hh;
+        a.inv_h = 1.0 / hh;
+        a.sigma = h->jvp_sigma;
+        if (mode == MODE_JVP) e = dispatch1d<cplx>(h->n, h->cfg.gas_law, h->cfg.riemann, a, s);
+        else e = dispatch1d<double>(h->n, h->cfg.gas_law, h->cfg.riemann, a, s);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "residual launch");
+    return FRSDG_OK;
+}
+} // namespace
+
+extern "C" {
+
+int frsdg_residual(frsdg_handle* h, double t, const double* U, double* R, void* stream)
+{
+    return run_residual(h, MODE_RESIDUAL, t, U, nullptr, R, stream);
+}
+
+int frsdg_rhs(frsdg_handle* h, double t, const double* U, double* rhs, void* stream)
+{
+    return run_residual(h, MODE_RHS, t, U, nullptr, rhs, stream);
+}
+
+int frsdg_ifunction(frsdg_handle* h, double t, const double* U, const double* U_t, double* F, void* stream)
+{
+    if (!U_t) return fail(FRSDG_ERR_ARG, "null U_t");
+    return run_residual(h, MODE_IFUNC, t, U, U_t, F, stream);
+}
+
+int frsdg_jvp_prepare(frsdg_handle* h, double t, double sigma, const double* U)
+{
+    if (!h || !U) return fail(FRSDG_ERR_ARG, "null argument");
+    h->jvp_t = t;
+    h->jvp_sigma = sigma;
+    h->jvp_U = U;
+    return FRSDG_OK;
+}
+
+int frsdg_jvp(frsdg_handle* h, const double* V, double* JV, void* stream)
+{
+    if (!h || !V) return fail(FRSDG_ERR_ARG, "null argument");
+    if (!h->jvp_U) return fail(FRSDG_ERR_ARG, "frsdg_jvp called before frsdg_jvp_prepare");
+    if (reinterpret_cast<uintptr_t>(V) & 15) return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
+    return run_residual(h, MODE_JVP, h->jvp_t, h->jvp_U, V, JV, stream);
+}
+
+int frsdg_post_step(frsdg_handle* h, double* U, void* stream)
+{
+    if (!h || !U) return fail(FRSDG_ERR_ARG, "null argument");
+    if (!h->cfg.apply_filter && !h->cfg.apply_weno) return FRSDG_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    h->last = s;
+    StabArgs a = h->st;
+    a.dst = U;
+    a.src = U;
+    if (h->d_work)
+    {
+        cudaError_t e = cudaMemcpyAsync(h->d_work, U, sizeof(double) * h->ntot, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return cuda_fail(e, "post-step copy");
+        a.src = h->d_work;
+    }
+    cudaError_t e = launch_stab(h->n, a, s);
+    if (e != cudaSuccess) return cuda_fail(e, "post-step launch");
+    return FRSDG_OK;
+}
+
+int frsdg_prim_to_cons(frsdg_handle* h, const double* prim, double* cons, void* stream)
+{
+    if (!h || !prim || !cons) return fail(FRSDG_ERR_ARG, "null argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    h->last = s;
+    cudaError_t e = launch_prim_to_cons(h->cfg.dim, h->n, h->nelem, prim, cons, s);
+    if (e != cudaSuccess) return cuda_fail(e, "prim_to_cons launch");
+    return FRSDG_OK;
+}
+
+int frsdg_rhs_host(frsdg_handle* h, double t, const double* U_host, double* rhs_host, void* stream)
+{
+    if (!h || !U_host || !rhs_host) return fail(FRSDG_ERR_ARG, "null argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!h->d_stage)
+    {
+        cudaError_t e = cudaMalloc(&h->d_stage, sizeof(double) * 2 * h->ntot);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(staging)");
+    }
+    const size_t bytes = sizeof(double) * h->ntot;
+    cudaError_t  e = cudaMemcpyAsync(h->d_stage, U_host, bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "H2D copy");
+    int rc = run_residual(h, MODE_RHS, t, h->d_stage, nullptr, h->d_stage + h->ntot, stream);
+    if (rc) return rc;
+    e = cudaMemcpyAsync(rhs_host, h->d_stage + h->ntot, bytes, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail(e, "D2H copy");
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "stream sync");
+    return FRSDG_OK;
+}
+
+int frsdg_status(frsdg_handle* h, int64_t* bad_nodes)
+{
+    if (!h || !bad_nodes) return fail(FRSDG_ERR_ARG, "null argument");
+    unsigned long long v = 0;
+    cudaError_t e = cudaStreamSynchronize(h->last);
+    if (e != cudaSuccess) return cuda_fail(e, "status sync");
+    e = cudaMemcpy(&v, h->d_bad, sizeof(v), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "status read");
+    e = cudaMemset(h->d_bad, 0, sizeof(v));
+    if (e != cudaSuccess) return cuda_fail(e, "status reset");
+    *bad_nodes = int64_t(v);
+    return FRSDG_OK;
+}
+
+} // extern "C"

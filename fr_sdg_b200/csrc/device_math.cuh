@@ -1,0 +1,129 @@
+// device_math.cuh -- scalar types of the residual kernels.
+//
+// The residual is templated on its scalar S:
+//   double  the FP64 residual (rhs_func / fun_implicit),
+//   cplx    complex FP64 for the complex-step JVP (matmult of the reference),
+//   float   the FP32 residual of the mixed-precision form.
+// cplx follows std::complex<double> semantics for finite values: principal-branch
+// sqrt, Smith's division (R. L. Smith, "Algorithm 116: Complex division",
+// CACM 5(8), 1962) and the textbook product.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace frsdg
+{
+
+struct __align__(16) cplx
+{
+    double re, im;
+    __host__ __device__ constexpr cplx() : re(0.0), im(0.0) {}
+    __host__ __device__ constexpr cplx(double r) : re(r), im(0.0) {}
+    __host__ __device__ constexpr cplx(double r, double i) : re(r), im(i) {}
+};
+
+__device__ __forceinline__ cplx operator+(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
+__device__ __forceinline__ cplx operator-(cplx a, cplx b) { return {a.re - b.re, a.im - b.im}; }
+__device__ __forceinline__ cplx operator-(cplx a) { return {-a.re, -a.im}; }
+__device__ __forceinline__ cplx operator*(cplx a, cplx b)
+{
+    return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+__device__ __forceinline__ cplx operator*(double s, cplx a) { return {s * a.re, s * a.im}; }
+__device__ __forceinline__ cplx operator*(cplx a, double s) { return {a.re * s, a.im * s}; }
+__device__ __forceinline__ cplx operator+(cplx a, double s) { return {a.re + s, a.im}; }
+__device__ __forceinline__ cplx operator+(double s, cplx a) { return {s + a.re, a.im}; }
+__device__ __forceinline__ cplx operator-(cplx a, double s) { return {a.re - s, a.im}; }
+__device__ __forceinline__ cplx operator-(double s, cplx a) { return {s - a.re, -a.im}; }
+__device__ __forceinline__ cplx operator/(cplx a, cplx b)
+{
+    // Smith's algorithm.
+    if (fabs(b.re) >= fabs(b.im))
+    {
+        const double r   = b.im / b.re;
+        const double den = b.re + b.im * r;
+        return {(a.re + a.im * r) / den, (a.im - a.re * r) / den};
+    }
+    const double r   = b.re / b.im;
+    const double den = b.re * r + b.im;
+    return {(a.re * r + a.im) / den, (a.im * r - a.re) / den};
+}
+__device__ __forceinline__ cplx operator/(cplx a, double s) { return {a.re / s, a.im / s}; }
+__device__ __forceinline__ cplx operator/(double s, cplx b) { return cplx(s) / b; }
+__device__ __forceinline__ cplx& operator+=(cplx& a, cplx b) { a = a + b; return a; }
+__device__ __forceinline__ cplx& operator-=(cplx& a, cplx b) { a = a - b; return a; }
+
+// ---- generic scalar functions -------------------------------------------
+__device__ __forceinline__ double s_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float s_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ cplx s_sqrt(cplx z)
+{
+    // principal branch, as C99 csqrt
+    if (z.re == 0.0 && z.im == 0.0) return {0.0, z.im};
+    const double t = sqrt(0.5 * (fabs(z.re) + hypot(z.re, z.im)));
+    if (z.re >= 0.0) return {t, z.im / (2.0 * t)};
+    return {fabs(z.im) / (2.0 * t), copysign(t, z.im)};
+}
+__device__ __forceinline__ double s_exp(double x) { return exp(x); }
+__device__ __forceinline__ float s_exp(float x) { return expf(x); }
+__device__ __forceinline__ cplx s_exp(cplx z)
+{
+    const double m = exp(z.re);
+    double       s, c;
+    sincos(z.im, &s, &c);
+    return {m * c, m * s};
+}
+
+// reciprocal: 1/x
+__device__ __forceinline__ double s_rcp(double x) { return 1.0 / x; }
+__device__ __forceinline__ float s_rcp(float x) { return 1.0f / x; }
+__device__ __forceinline__ cplx s_rcp(cplx z) { return cplx(1.0) / z; }
+
+// real part, and the value the HLLC branch tests (riemann_solver.hpp:149-155:
+// Re + Im for complex, the value itself for real scalars).
+__device__ __forceinline__ double s_re(double x) { return x; }
+__device__ __forceinline__ double s_re(float x) { return x; }
+__device__ __forceinline__ double s_re(cplx z) { return z.re; }
+__device__ __forceinline__ double s_im(cplx z) { return z.im; }
+__device__ __forceinline__ double s_branch(double x) { return x; }
+__device__ __forceinline__ double s_branch(float x) { return x; }
+__device__ __forceinline__ double s_branch(cplx z) { return z.re + z.im; }
+
+// wrap_positive (macro_and_libc.hpp:117-138): max(DBL_MIN, rho); for complex, the
+// real part decides and a clamped value loses its imaginary part.
+__device__ __forceinline__ double s_wrap_positive(double r)
+{
+    const double floor = 2.2250738585072014e-308; // DBL_MIN
+    return fmax(floor, r);
+}
+__device__ __forceinline__ float s_wrap_positive(float r)
+{
+    const float floor = 1.17549435e-38f; // FLT_MIN
+    return fmaxf(floor, r);
+}
+__device__ __forceinline__ cplx s_wrap_positive(cplx r)
+{
+    const double floor = 2.2250738585072014e-308;
+    return (r.re < floor) ? cplx(floor, 0.0) : r;
+}
+
+template <class S> __device__ __forceinline__ S s_select(bool c, S a, S b) { return c ? a : b; }
+
+template <class S> struct scalar_traits;
+template <> struct scalar_traits<double>
+{
+    using real = double;
+    static constexpr int words = 1;
+};
+template <> struct scalar_traits<float>
+{
+    using real = float;
+    static constexpr int words = 1;
+};
+template <> struct scalar_traits<cplx>
+{
+    using real = double;
+    static constexpr int words = 2;
+};
+
+} // namespace frsdg

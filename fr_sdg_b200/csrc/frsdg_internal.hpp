@@ -1,0 +1,106 @@
+// frsdg_internal.hpp -- structures shared by the C-ABI host code and the kernels.
+#pragma once
+#include "../../include/frsdg.h"
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace frsdg
+{
+
+constexpr int kMaxN = 10;  // p <= 9
+constexpr int kThreads = 256;
+
+// Output forms of one residual pass (the PETSc callback each one serves).
+enum Mode : int
+{
+    MODE_RESIDUAL = 0, // R(U)                      residual_kernel<double>
+    MODE_RHS      = 1, // -R(U)                     rhs_func
+    MODE_IFUNC    = 2, // U_t + R(M(U))             fun_implicit
+    MODE_JVP      = 3  // sigma Im(u)/h + Im(R)/h   ComplexStepJacobianStrategy::matmult
+};
+
+// Geometry classes of the 2D kernel: constant diagonal metrics (Cartesian and the
+// straight de Laval channel) or cached per-node metrics and per-face normals.
+enum GeoClass : int
+{
+    GEO_AFFINE = 0,
+    GEO_CURVED = 1
+};
+
+struct BcDev
+{
+    int32_t kind;
+    int32_t pad_;
+    double  state[4];
+    double  params[6];
+};
+
+// Small per-handle operators: differentiation matrix, VCJH correction derivatives.
+struct Ops
+{
+    double D[kMaxN * kMaxN];
+    double dL[kMaxN];
+    double dR[kMaxN];
+    double csi[kMaxN];
+};
+
+struct GasParams
+{
+    double gamma, a, b;
+};
+
+struct Fr2dArgs
+{
+    int    Nx, Ny, per_x, per_y;
+    GasParams gas;
+    double xi_x, xi_y, eta_x, eta_y, scale_x, scale_y; // GEO_AFFINE
+    const double* metrics;                              // GEO_CURVED: [elem][node][4] xi_x, xi_y, eta_x, eta_y
+    const double* xnorm;                                // GEO_CURVED: [(j*(Nx+1)+I)*n + l][2]
+    const double* ynorm;                                // GEO_CURVED: [(J*Nx+i)*n + k][2]
+    const double* bxy[4];                               // boundary face points [idx][2], by direction
+    BcDev  bc[4];
+    double Lx, Ly;
+    double t;
+    int    mode, cond_sys;
+    const double* U;   // state (primitive when cond_sys)
+    const double* W;   // JVP: direction V; IFUNC: U_t
+    void*  out;        // double* (float* for the FP32 residual)
+    double h, inv_h, sigma;
+    unsigned long long* bad;
+    Ops    ops;
+};
+
+struct Fr1dArgs
+{
+    int    N, per;
+    GasParams gas;
+    double inv_jac, h_elem;
+    int    radial;
+    BcDev  bc[2];
+    double t;
+    int    mode, cond_sys;
+    const double* U;
+    const double* W;
+    void*  out;
+    double h, inv_h, sigma;
+    unsigned long long* bad;
+    Ops    ops;
+};
+
+// Tile of elements per CTA of the 2D kernel: TX along x (contiguous in memory)
+// by TY along y, about 200-400 nodes per tile.
+__host__ __device__ constexpr int tile_x(int n)
+{
+    return n <= 2 ? 8 : n <= 3 ? 8 : n <= 4 ? 4 : n <= 6 ? 4 : 2;
+}
+__host__ __device__ constexpr int tile_y(int n)
+{
+    return n <= 2 ? 8 : n <= 3 ? 4 : n <= 4 ? 4 : n <= 6 ? 2 : n <= 9 ? 2 : 1;
+}
+
+// Launchers (one translation unit per polynomial order).
+template <class S, int N> cudaError_t launch_fr2d(int gas, int riem, int geo, const Fr2dArgs& a, cudaStream_t s);
+template <class S, int N> cudaError_t launch_fr1d(int gas, int riem, const Fr1dArgs& a, cudaStream_t s);
+
+} // namespace frsdg

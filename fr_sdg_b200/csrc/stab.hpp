@@ -1,0 +1,26 @@
+// stab.hpp -- launch interface of the post-step stabilisation and the change of
+// variables kernels.
+#pragma once
+#include "frsdg_internal.hpp"
+
+namespace frsdg
+{
+
+struct StabArgs
+{
+    int    dim, Nx, Ny, per_x, per_y;
+    int    apply_filter, apply_weno;
+    double gam[3];        // WENO linear weights ((1-g)/2, g, (1-g)/2)
+    double one_over_norm; // shock-sensor normalisation (filter.hpp:646-652)
+    double theta, threshold;
+    double F[kMaxN * kMaxN];
+    double D[kMaxN * kMaxN];
+    double w[kMaxN];
+    const double* src;
+    double*       dst;
+};
+
+cudaError_t launch_stab(int n, const StabArgs& a, cudaStream_t s);
+cudaError_t launch_prim_to_cons(int dim, int n, int64_t nelem, const double* in, double* out, cudaStream_t s);
+
+} // namespace frsdg

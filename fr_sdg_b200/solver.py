@@ -1,0 +1,103 @@
+"""FRSolver: the reference's PETSc callback surface over libfrsdg.
+
+Method names follow PetscSolver and ComplexStepJacobianStrategy
+(include/petsc_solver_impl.hpp): rhs_func (657-670), fun_implicit (626-655),
+pre_jv_eval (223-248), matmult (250-267), apply_stabilization (683-702) and
+primitive_to_conservative (719-727), plus residual_kernel
+(physics_impl_2D.hpp:646-902).  Vectors are torch float64 CUDA tensors in the
+DMDA natural layout; every call is ordered on torch's current CUDA stream.
+Errors raise FrsdgError with the library's message, like PetscCall.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import _abi as A
+
+
+def _ptr(t: torch.Tensor) -> int:
+    return t.data_ptr()
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+class FRSolver:
+    def __init__(self, cfg: A.frsdg_config):
+        self.cfg = cfg
+        self._lib = A.lib()
+        h = C.c_void_p()
+        A.check(self._lib.frsdg_create(C.byref(cfg), C.byref(h)), "frsdg_create")
+        self._h = h
+        n = C.c_int64()
+        A.check(self._lib.frsdg_n_dofs(h, C.byref(n)), "frsdg_n_dofs")
+        self.n_dofs = int(n.value)
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self) -> None:
+        if self._h:
+            self._lib.frsdg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check_vec(self, *vs: torch.Tensor) -> None:
+        for v in vs:
+            if v.dtype != torch.float64 or not v.is_cuda or not v.is_contiguous() or v.numel() != self.n_dofs:
+                raise ValueError(f"expected a contiguous float64 CUDA vector of {self.n_dofs} entries")
+
+    # -- PETSc callbacks --------------------------------------------------
+    def residual_kernel(self, t: float, U: torch.Tensor, R: torch.Tensor) -> None:
+        self._check_vec(U, R)
+        A.check(self._lib.frsdg_residual(self._h, t, _ptr(U), _ptr(R), _stream()), "frsdg_residual")
+
+    def rhs_func(self, t: float, U: torch.Tensor, rhs: torch.Tensor) -> None:
+        self._check_vec(U, rhs)
+        A.check(self._lib.frsdg_rhs(self._h, t, _ptr(U), _ptr(rhs), _stream()), "frsdg_rhs")
+
+    def fun_implicit(self, t: float, U: torch.Tensor, U_t: torch.Tensor, F: torch.Tensor) -> None:
+        self._check_vec(U, U_t, F)
+        A.check(self._lib.frsdg_ifunction(self._h, t, _ptr(U), _ptr(U_t), _ptr(F), _stream()), "frsdg_ifunction")
+
+    def pre_jv_eval(self, t: float, U: torch.Tensor, sigma: float) -> None:
+        self._check_vec(U)
+        self._jvp_U = U  # keep alive while the library holds the pointer
+        A.check(self._lib.frsdg_jvp_prepare(self._h, t, sigma, _ptr(U)), "frsdg_jvp_prepare")
+
+    def matmult(self, v: torch.Tensor, out: torch.Tensor) -> None:
+        self._check_vec(v, out)
+        A.check(self._lib.frsdg_jvp(self._h, _ptr(v), _ptr(out), _stream()), "frsdg_jvp")
+
+    def apply_stabilization(self, U: torch.Tensor) -> None:
+        self._check_vec(U)
+        A.check(self._lib.frsdg_post_step(self._h, _ptr(U), _stream()), "frsdg_post_step")
+
+    def primitive_to_conservative(self, inp: torch.Tensor, out: torch.Tensor) -> None:
+        self._check_vec(inp, out)
+        A.check(self._lib.frsdg_prim_to_cons(self._h, _ptr(inp), _ptr(out), _stream()), "frsdg_prim_to_cons")
+
+    def rhs_func_host(self, t: float, U_host: torch.Tensor, rhs_host: torch.Tensor) -> None:
+        """rhs_func on host (ideally pinned) float64 tensors; returns when done."""
+        for v in (U_host, rhs_host):
+            if v.dtype != torch.float64 or v.is_cuda or not v.is_contiguous() or v.numel() != self.n_dofs:
+                raise ValueError("expected contiguous float64 host vectors")
+        A.check(self._lib.frsdg_rhs_host(self._h, t, _ptr(U_host), _ptr(rhs_host), _stream()), "frsdg_rhs_host")
+
+    def status(self) -> int:
+        """Nodes with non-positive or non-finite density seen since the last call."""
+        n = C.c_int64()
+        A.check(self._lib.frsdg_status(self._h, C.byref(n)), "frsdg_status")
+        return int(n.value)

@@ -1,0 +1,204 @@
+/*
+ * frsdg.h -- C ABI of the B200 Flux Reconstruction residual library (libfrsdg.so).
+ *
+ * The library replaces the hot path of fr_sdg's PETSc time-stepping callbacks:
+ * the FR spatial residual of the compressible Euler equations, its complex-step
+ * Jacobian-vector product, the post-step stabilisation and the change of
+ * variables.  Every entry point takes plain pointers and sizes; no PETSc, CUDA
+ * or torch type appears in a signature.  Streams are passed as `void*`
+ * (a cudaStream_t, NULL = legacy default stream).
+ *
+ * Vector layout (the DMDA natural ordering of a single-rank PETSc Vec,
+ * include/vec_dof_view.hpp:102-117 and include/physics_impl_2D.hpp:13-35):
+ *   2D: element (i,j) starts at ((j*Nx + i) * ndofs), ndofs = 4*n*n, and inside an
+ *       element value (eq, k, l) sits at ((l*n + k)*4 + eq)   [node-major AoS]
+ *   1D: element e starts at (e * ndofs), ndofs = 3*n, and inside an element value
+ *       (eq, node) sits at (eq*n + node)                        [SoA]
+ * with n = poly_deg + 1 GLL points per direction.
+ *
+ * Every function returns 0 (FRSDG_OK) on success or a negative FRSDG_ERR_* code;
+ * frsdg_last_error() gives a one-line description of the last failure on the
+ * calling thread.  Device pointers must be 16-byte aligned.  A handle is not
+ * thread safe: use one handle per host thread.  Hot calls (residual, rhs,
+ * ifunction, jvp, post_step, prim_to_cons) allocate nothing; every workspace is
+ * allocated by frsdg_create.
+ */
+#ifndef FRSDG_H
+#define FRSDG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FRSDG_ABI_VERSION 1
+
+/* ---- status codes (PETSc-style: 0 = success) ---------------------------- */
+enum {
+    FRSDG_OK             = 0,
+    FRSDG_ERR_ARG        = -1, /* invalid argument or configuration */
+    FRSDG_ERR_CUDA       = -2, /* a CUDA runtime call failed */
+    FRSDG_ERR_NOMEM      = -3, /* device allocation failed in frsdg_create */
+    FRSDG_ERR_UNSUPPORTED = -4, /* configuration valid but not built in */
+    FRSDG_ERR_NODEVICE   = -5  /* no CUDA device visible */
+};
+
+/* ---- policy enums (runtime stand-ins for the reference's compile-time traits,
+ *      include/physics_evaluator.hpp:37-52) ------------------------------- */
+enum { FRSDG_GAS_IDEAL = 0, FRSDG_GAS_VDW = 1 };              /* gas_models.hpp:56-158 */
+enum { FRSDG_RUSANOV = 0, FRSDG_HLLC = 1 };                    /* riemann_solver.hpp:13-17 */
+enum { FRSDG_COORD_CARTESIAN = 0, FRSDG_COORD_RADIAL = 1 };    /* macro_and_libc.hpp:154-159 */
+
+/* Geometry policies (geometry_models.hpp:61-195, tests/bump.cpp:13-171):
+ *  CARTESIAN     x = Lx*csi, y = Ly*eta
+ *  DELAVAL       GeometryDeLavalNozzle2D with the straight-line profile (h=0.5, h'=0)
+ *  WALL_PROFILE  x = x0 + Lx*csi, y = h(x)*(1-eta) + Ly*eta with a wall profile h(x)
+ *                chosen by geom_profile (wedges of tests/bump.cpp and
+ *                tests/boundary_conforming.cpp, or a Gaussian bump)
+ *  SINE_WARP     x = Lx*csi + A sin(2 pi csi) sin(2 pi eta), same displacement on y */
+enum {
+    FRSDG_GEOM_CARTESIAN    = 0,
+    FRSDG_GEOM_DELAVAL      = 1,
+    FRSDG_GEOM_WALL_PROFILE = 2,
+    FRSDG_GEOM_SINE_WARP    = 3
+};
+enum {
+    FRSDG_PROFILE_FLAT        = 0, /* h = 0 */
+    FRSDG_PROFILE_WEDGE_BUMP  = 1, /* tests/bump.cpp:29-119 (5 zones, returns -h) */
+    FRSDG_PROFILE_WEDGE_BC    = 2, /* tests/boundary_conforming.cpp:28-67 (3 zones) */
+    FRSDG_PROFILE_GAUSS_BUMP  = 3  /* h = A exp(-k x^2), geom_params[1]=A, [2]=k */
+};
+
+/* Boundary faces, in the reference's Direction order (boundary_conditions.hpp:17-23). */
+enum { FRSDG_LEFT = 0, FRSDG_RIGHT = 1, FRSDG_TOP = 2, FRSDG_BOTTOM = 3 };
+
+/* Boundary kinds.  OUTFLOW, WALL and PERIODIC are the reference's native binders
+ * (boundary_conditions.hpp:296-323) and keep the imaginary part in the complex
+ * step; every other kind stands for a user lambda (bind_lambda, 270-294) and,
+ * like it, sees only the real part of the interior state in the complex step. */
+enum {
+    FRSDG_BC_OUTFLOW         = 0, /* ghost = interior */
+    FRSDG_BC_WALL            = 1, /* flip the momentum component of the face axis */
+    FRSDG_BC_PERIODIC        = 2, /* wrap to the opposite element (both faces of an axis) */
+    FRSDG_BC_DIRICHLET       = 3, /* ghost = state[0..3] (conservative) */
+    FRSDG_BC_SLIP_WALL       = 4, /* reflect velocity about the face normal (tests/bump.cpp:250-272) */
+    FRSDG_BC_VORTEX          = 5, /* exact isentropic vortex (factory.hpp:311-352, 504-511);
+                                     params: u0, v0, beta, r_v, l */
+    FRSDG_BC_SUBSONIC_INFLOW = 6, /* total pressure / temperature inflow; params: p0, T0, R, angle */
+    FRSDG_BC_PRESSURE_OUTLET = 7  /* static pressure outlet; params: p_out */
+};
+
+typedef struct frsdg_bc {
+    int32_t kind;
+    int32_t pad_;
+    double  state[4];  /* conservative ghost for DIRICHLET (1D uses state[0..2]) */
+    double  params[6];
+} frsdg_bc;
+
+/* Mirror of the ConfigOptions fields the hot path reads (parser.hpp:45-191),
+ * plus the policy choices the reference fixes at compile time. */
+typedef struct frsdg_config {
+    int32_t dim;             /* 1 or 2 */
+    int32_t poly_deg;        /* p, 1..9 (n = p+1 GLL points per direction) */
+    int32_t n_elems[2];      /* Nx, Ny (Ny ignored in 1D) */
+    double  box_length[2];   /* Lx, Ly */
+    double  radau_corr;      /* VCJH c (0 = nodal DG) */
+    int32_t gas_law;         /* FRSDG_GAS_* */
+    int32_t riemann;         /* FRSDG_RUSANOV / FRSDG_HLLC */
+    double  gamma, R_spec, vdw_a, vdw_b;
+    int32_t coord_sys;       /* FRSDG_COORD_* (RADIAL: 1D only) */
+    int32_t geometry;        /* FRSDG_GEOM_* (2D only) */
+    int32_t geom_profile;    /* FRSDG_PROFILE_* for WALL_PROFILE */
+    int32_t pad0_;
+    double  geom_params[4];  /* WALL_PROFILE: [0]=x0; SINE_WARP: [0]=amplitude */
+    frsdg_bc bc[4];          /* indexed by FRSDG_LEFT..FRSDG_BOTTOM (1D: LEFT, RIGHT) */
+    /* stabilisation (filter.hpp:393-759) */
+    int32_t apply_filter;
+    int32_t filt_cut_off;    /* default 2 */
+    int32_t filt_strength;   /* default 32 */
+    int32_t apply_weno;
+    double  filt_alpha;      /* default 36 */
+    double  weno_gamma;      /* default 0.998 */
+    double  shock_theta;     /* default 1 */
+    double  shock_threshold; /* default 0.8 */
+    int32_t cond_sys;        /* -solve_positive_preserving: unknowns (log rho, u, [v], log e) */
+    int32_t pad1_;
+    double  csd_eps;         /* complex-step h (reference: 1e-7, petsc_solver_impl.hpp:179) */
+} frsdg_config;
+
+typedef struct frsdg_handle frsdg_handle;
+
+/* Library identity and errors. */
+int         frsdg_abi_version(void);
+const char* frsdg_last_error(void);
+
+/* Fill *cfg with the reference defaults (parser.hpp:45-91, 257-275). */
+int frsdg_config_default(frsdg_config* cfg);
+
+/* Build a handle on the current CUDA device: reference element (GLL nodes,
+ * differentiation matrix, VCJH correction derivatives), filter matrices, cached
+ * curved metrics and face normals, boundary data and all workspaces.
+ * Replaces PhysicsEvaluator's constructor (physics_evaluator.hpp:188-201) and
+ * PetscSolver::setup_dmda/setup_ts (petsc_solver_impl.hpp:492-612). */
+int frsdg_create(const frsdg_config* cfg, frsdg_handle** out);
+int frsdg_destroy(frsdg_handle* h);
+
+/* Number of doubles in one solution vector (Nx*Ny*4*n*n or Nx*3*n). */
+int frsdg_n_dofs(const frsdg_handle* h, int64_t* n);
+
+/* R(U): PhysicsEvaluator::residual_kernel<double> (physics_impl_2D.hpp:646-902,
+ * physics_impl_1D.hpp:9-94).  U and R are device pointers. */
+int frsdg_residual(frsdg_handle* h, double t, const double* U, double* R, void* stream);
+
+/* rhs = -R(U): PetscSolver::rhs_func (petsc_solver_impl.hpp:657-670). */
+int frsdg_rhs(frsdg_handle* h, double t, const double* U, double* rhs, void* stream);
+
+/* F = U_t + R(M(U)): PetscSolver::fun_implicit (petsc_solver_impl.hpp:626-655);
+ * M = prim->cons when cond_sys, identity otherwise. */
+int frsdg_ifunction(frsdg_handle* h, double t, const double* U, const double* U_t,
+                    double* F, void* stream);
+
+/* Snapshot (t, sigma, U) for later frsdg_jvp calls:
+ * ComplexStepJacobianStrategy::pre_jv_eval (petsc_solver_impl.hpp:223-248).
+ * U must stay valid until the next frsdg_jvp_prepare. */
+int frsdg_jvp_prepare(frsdg_handle* h, double t, double sigma, const double* U);
+
+/* JV = sigma*Im(M(U+ihV))/h + Im(R(M(U+ihV)))/h, h = cfg.csd_eps:
+ * ComplexStepJacobianStrategy::matmult (petsc_solver_impl.hpp:250-432). */
+int frsdg_jvp(frsdg_handle* h, const double* V, double* JV, void* stream);
+
+/* In-place post-step stabilisation U <- limit(U) (spectral filter, WENO with
+ * shock sensor): PetscSolver::apply_stabilization (petsc_solver_impl.hpp:683-702). */
+int frsdg_post_step(frsdg_handle* h, double* U, void* stream);
+
+/* cons = M(prim): PetscSolver::primitive_to_conservative (petsc_solver_impl.hpp:719-727). */
+int frsdg_prim_to_cons(frsdg_handle* h, const double* prim, double* cons, void* stream);
+
+/* rhs = -R(U) with U and rhs in host memory; the copies to and from the device
+ * use handle-owned staging buffers on `stream` and the call returns after the
+ * result is in host memory.  For callers whose PETSc Vecs live on the host. */
+int frsdg_rhs_host(frsdg_handle* h, double t, const double* U_host, double* rhs_host,
+                   void* stream);
+
+/* Device-side health word: number of nodes seen with a non-positive or
+ * non-finite density by the last residual call (0 = healthy).  Synchronises the
+ * handle's last stream. */
+int frsdg_status(frsdg_handle* h, int64_t* bad_nodes);
+
+/* Host-only set-up operators, usable without a GPU.
+ * Reference element: GLL (reference_element.hpp:50-147) and CachedElementData
+ * (cached_computations.hpp:225-334).  Arrays: nodes[n], weights[n], D[n*n]
+ * (row-major D(i,j)), dL[n], dR[n] with n = p+1. */
+int frsdg_reference_element(int32_t p, double radau_corr, double* nodes, double* weights,
+                            double* D, double* dL, double* dR);
+
+/* Spectral filter matrix V diag(sigma) V^-1 (filter.hpp:451-484), row-major n*n. */
+int frsdg_filter_matrix(int32_t p, int32_t cut_off, int32_t strength, double alpha,
+                        double* F);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FRSDG_H */

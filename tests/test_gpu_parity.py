@@ -1,0 +1,235 @@
+"""GPU parity: libfrsdg through its C ABI against the CPU oracle on seeded inputs.
+
+Bar: max|gpu - oracle| / max|oracle| <= 1e-12 for the FP64 residual forms
+(R, -R, U_t + R), the post-step stabilisation and the change of variables, and
+<= 1e-11 for the complex-step JVP.
+"""
+import zlib
+
+import numpy as np
+import pytest
+import torch
+
+from fr_sdg_b200 import FRSolver
+from fr_sdg_b200 import _abi as A
+from fr_sdg_b200.workloads import make_config
+from oracle.oracle import Oracle
+from tests.helpers import TOL_FP64, TOL_JVP, cons_to_prim, random_state, rel_err
+
+pytestmark = pytest.mark.gpu
+
+PER = (A.BC_PERIODIC, None, None)
+OUT = A.BC_OUTFLOW
+
+
+def _cfg2d(**kw):
+    base = dict(dim=2, p=3, n_elems=(7, 5), box=(1.3, 0.9), riemann="hllc",
+                bcs={A.LEFT: OUT, A.RIGHT: OUT, A.TOP: OUT, A.BOTTOM: OUT})
+    base.update(kw)
+    return make_config(**base)
+
+
+VDW = dict(gas="vdw", vdw=(0.05, 0.02))
+VORTEX = (A.BC_VORTEX, None, (1.0, 1.0, 5.0, 1.0, 10.0))
+
+CASES_2D = {
+    "cart_ideal_rusanov_p3": dict(riemann="rusanov"),
+    "cart_ideal_hllc_p1_periodic": dict(p=1, n_elems=(9, 6), bcs={A.LEFT: PER, A.RIGHT: PER, A.TOP: PER, A.BOTTOM: PER}),
+    "cart_ideal_hllc_p2": dict(p=2, n_elems=(11, 9)),
+    "cart_vdw_hllc_p4_walls": dict(p=4, **VDW, bcs={A.LEFT: A.BC_WALL, A.RIGHT: OUT, A.TOP: A.BC_WALL, A.BOTTOM: OUT}),
+    "cart_vdw_rusanov_p5_perx": dict(p=5, riemann="rusanov", **VDW,
+                                     bcs={A.LEFT: PER, A.RIGHT: PER, A.TOP: A.BC_WALL, A.BOTTOM: A.BC_WALL}),
+    "cart_ideal_hllc_p6": dict(p=6, n_elems=(5, 5), radau_corr=0.01),
+    "cart_ideal_hllc_p7": dict(p=7, n_elems=(3, 5)),
+    "cart_vdw_hllc_p8_periodic": dict(p=8, n_elems=(4, 3), **VDW, bcs={A.LEFT: PER, A.RIGHT: PER, A.TOP: PER, A.BOTTOM: PER}),
+    "cart_ideal_rusanov_p9": dict(p=9, n_elems=(3, 2), riemann="rusanov"),
+    "sinewarp_hllc_p4_periodic": dict(p=4, n_elems=(6, 6), box=(10.0, 10.0), geometry=A.GEOM_SINE_WARP,
+                                      geom_params=(0.1, 0, 0, 0),
+                                      bcs={A.LEFT: PER, A.RIGHT: PER, A.TOP: PER, A.BOTTOM: PER}),
+    "sinewarp_vdw_rusanov_p3": dict(p=3, n_elems=(5, 7), box=(2.0, 3.0), geometry=A.GEOM_SINE_WARP,
+                                    geom_params=(0.05, 0, 0, 0), riemann="rusanov", **VDW,
+                                    bcs={A.LEFT: PER, A.RIGHT: PER, A.TOP: A.BC_WALL, A.BOTTOM: OUT}),
+    "bump_hllc_p3_inflow_outlet": dict(p=3, n_elems=(12, 4), box=(3.0, 0.8), geometry=A.GEOM_WALL_PROFILE,
+                                       profile=A.PROFILE_GAUSS_BUMP, geom_params=(-1.5, 0.0625, 25.0, 0.0),
+                                       bcs={A.LEFT: (A.BC_SUBSONIC_INFLOW, None, (1.0, 1.0, 1.0, 0.0)),
+                                            A.RIGHT: (A.BC_PRESSURE_OUTLET, None, (0.84,)),
+                                            A.BOTTOM: A.BC_SLIP_WALL, A.TOP: A.BC_SLIP_WALL}),
+    "wedge_bump_rusanov_p2_dirichlet": dict(p=2, n_elems=(10, 5), geometry=A.GEOM_WALL_PROFILE,
+                                            profile=A.PROFILE_WEDGE_BUMP, riemann="rusanov",
+                                            bcs={A.LEFT: (A.BC_DIRICHLET, (1.0, 2.0, 0.0, 4.5), None),
+                                                 A.TOP: (A.BC_DIRICHLET, (1.0, 2.0, 0.0, 4.5), None),
+                                                 A.RIGHT: OUT, A.BOTTOM: A.BC_SLIP_WALL}),
+    "wedge_bc_hllc_p3": dict(p=3, n_elems=(8, 4), geometry=A.GEOM_WALL_PROFILE, profile=A.PROFILE_WEDGE_BC,
+                             bcs={A.LEFT: OUT, A.RIGHT: OUT, A.TOP: A.BC_WALL, A.BOTTOM: A.BC_SLIP_WALL}),
+    "delaval_hllc_p3": dict(p=3, geometry=A.GEOM_DELAVAL, bcs={A.LEFT: OUT, A.RIGHT: OUT, A.TOP: A.BC_WALL,
+                                                                A.BOTTOM: A.BC_WALL}),
+    "vortex_dirichlet_p3": dict(p=3, n_elems=(6, 6), box=(10.0, 10.0),
+                                bcs={A.LEFT: VORTEX, A.RIGHT: VORTEX, A.TOP: PER, A.BOTTOM: PER}),
+    "vdw_pressure_outlet_p4": dict(p=4, n_elems=(6, 4), **VDW,
+                                   bcs={A.LEFT: OUT, A.RIGHT: (A.BC_PRESSURE_OUTLET, None, (0.9,)),
+                                        A.TOP: A.BC_WALL, A.BOTTOM: A.BC_WALL}),
+}
+
+
+def _dev(a, cuda):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(cuda)
+
+
+@pytest.fixture(scope="module", params=sorted(CASES_2D))
+def case2d(request):
+    cfg = _cfg2d(**CASES_2D[request.param])
+    return request.param, cfg
+
+
+def test_residual_2d(case2d, cuda):
+    name, cfg = case2d
+    U = random_state(cfg, seed=zlib.crc32(name.encode()) % 1000)
+    t = 0.7
+    ref = Oracle(cfg, threads=4).residual(t, U)
+    with FRSolver(cfg) as s:
+        Ud = _dev(U, cuda)
+        R = torch.empty_like(Ud)
+        s.residual_kernel(t, Ud, R)
+        got = R.cpu().numpy()
+        assert s.status() == 0
+    err = rel_err(got, ref)
+    assert err <= TOL_FP64, f"{name}: rel err {err:.3e}"
+
+
+def test_rhs_and_ifunction_2d(case2d, cuda):
+    name, cfg = case2d
+    U = random_state(cfg, seed=7 + zlib.crc32(name.encode()) % 97, smooth=True)
+    Udot = np.random.default_rng(3).normal(size=U.size)
+    o = Oracle(cfg, threads=4)
+    with FRSolver(cfg) as s:
+        Ud, Ut = _dev(U, cuda), _dev(Udot, cuda)
+        F = torch.empty_like(Ud)
+        s.rhs_func(0.3, Ud, F)
+        assert rel_err(F.cpu().numpy(), o.rhs(0.3, U)) <= TOL_FP64
+        s.fun_implicit(0.3, Ud, Ut, F)
+        assert rel_err(F.cpu().numpy(), o.ifunction(0.3, U, Udot)) <= TOL_FP64
+
+
+def test_jvp_2d(case2d, cuda):
+    name, cfg = case2d
+    U = random_state(cfg, seed=11)
+    V = np.random.default_rng(5).normal(size=U.size)
+    for h in (1e-7, 1e-30):
+        cfg.csd_eps = h
+        ref = Oracle(cfg, threads=4).jvp(0.2, 2.5, U, V)
+        with FRSolver(cfg) as s:
+            Ud, Vd = _dev(U, cuda), _dev(V, cuda)
+            JV = torch.empty_like(Ud)
+            s.pre_jv_eval(0.2, Ud, 2.5)
+            s.matmult(Vd, JV)
+            err = rel_err(JV.cpu().numpy(), ref)
+        assert err <= TOL_JVP, f"{name} h={h}: rel err {err:.3e}"
+
+
+@pytest.mark.parametrize("name", ["cart_ideal_hllc_p2", "sinewarp_hllc_p4_periodic", "cart_vdw_hllc_p4_walls"])
+def test_change_of_variables_2d(name, cuda):
+    cfg = _cfg2d(**CASES_2D[name])
+    cfg.cond_sys = 1
+    Uc = random_state(cfg, seed=21, smooth=True)
+    P = cons_to_prim(cfg, Uc)
+    Udot = np.random.default_rng(9).normal(size=P.size)
+    V = np.random.default_rng(10).normal(size=P.size)
+    o = Oracle(cfg, threads=4)
+    with FRSolver(cfg) as s:
+        Pd, Ut, Vd = _dev(P, cuda), _dev(Udot, cuda), _dev(V, cuda)
+        out = torch.empty_like(Pd)
+        s.primitive_to_conservative(Pd, out)
+        assert rel_err(out.cpu().numpy(), o.prim_to_cons(P)) <= TOL_FP64
+        s.fun_implicit(0.1, Pd, Ut, out)
+        assert rel_err(out.cpu().numpy(), o.ifunction(0.1, P, Udot)) <= TOL_FP64
+        for h in (1e-7, 1e-30):
+            cfg.csd_eps = h
+            with FRSolver(cfg) as s2:
+                s2.pre_jv_eval(0.1, Pd, 1.5)
+                s2.matmult(Vd, out)
+                assert rel_err(out.cpu().numpy(), Oracle(cfg).jvp(0.1, 1.5, P, V)) <= TOL_JVP
+
+
+@pytest.mark.parametrize("stab", ["filter", "weno", "both"])
+@pytest.mark.parametrize("name", ["cart_ideal_rusanov_p3", "cart_vdw_rusanov_p5_perx", "sinewarp_hllc_p4_periodic"])
+def test_post_step_2d(name, stab, cuda):
+    kw = dict(CASES_2D[name])
+    kw.update(apply_filter=stab in ("filter", "both"), apply_weno=stab in ("weno", "both"), threshold=0.3)
+    cfg = _cfg2d(**kw)
+    U = random_state(cfg, seed=31)
+    ref = Oracle(cfg).post_step(U)
+    with FRSolver(cfg) as s:
+        Ud = _dev(U, cuda)
+        s.apply_stabilization(Ud)
+        got = Ud.cpu().numpy()
+    err = rel_err(got, ref)
+    assert err <= TOL_FP64, f"{name}/{stab}: rel err {err:.3e}"
+
+
+# ---------------------------------------------------------------- 1D
+CASES_1D = {
+    "sod_rusanov_p3": dict(p=3, n_elems=(40, 1), riemann="rusanov", apply_filter=True),
+    "hllc_p2_periodic": dict(p=2, n_elems=(33, 1), riemann="hllc", bcs={A.LEFT: PER, A.RIGHT: PER}),
+    "vdw_hllc_p5_walls": dict(p=5, n_elems=(37, 1), riemann="hllc", **VDW, bcs={A.LEFT: A.BC_WALL, A.RIGHT: A.BC_WALL}),
+    "dirichlet_rusanov_p4": dict(p=4, n_elems=(20, 1), riemann="rusanov",
+                                 bcs={A.LEFT: (A.BC_DIRICHLET, (1.0, 0.2, 2.6), None), A.RIGHT: OUT}),
+    "radial_hllc_p3": dict(p=3, n_elems=(50, 1), riemann="hllc", coord_sys=A.COORD_RADIAL,
+                           bcs={A.LEFT: A.BC_WALL, A.RIGHT: OUT}),
+    "p9_rusanov": dict(p=9, n_elems=(9, 1), riemann="rusanov"),
+    "p1_hllc_periodic": dict(p=1, n_elems=(70, 1), riemann="hllc", bcs={A.LEFT: PER, A.RIGHT: PER}),
+}
+
+
+@pytest.fixture(scope="module", params=sorted(CASES_1D))
+def case1d(request):
+    kw = dict(dim=1, box=(1.0, 1.0), bcs={A.LEFT: OUT, A.RIGHT: OUT})
+    kw.update(CASES_1D[request.param])
+    return request.param, make_config(**kw)
+
+
+def test_residual_1d(case1d, cuda):
+    name, cfg = case1d
+    U = random_state(cfg, seed=41)
+    Udot = np.random.default_rng(2).normal(size=U.size)
+    V = np.random.default_rng(4).normal(size=U.size)
+    o = Oracle(cfg)
+    with FRSolver(cfg) as s:
+        Ud, Ut, Vd = _dev(U, cuda), _dev(Udot, cuda), _dev(V, cuda)
+        out = torch.empty_like(Ud)
+        s.residual_kernel(0.0, Ud, out)
+        assert rel_err(out.cpu().numpy(), o.residual(0.0, U)) <= TOL_FP64, name
+        s.rhs_func(0.0, Ud, out)
+        assert rel_err(out.cpu().numpy(), o.rhs(0.0, U)) <= TOL_FP64, name
+        s.fun_implicit(0.0, Ud, Ut, out)
+        assert rel_err(out.cpu().numpy(), o.ifunction(0.0, U, Udot)) <= TOL_FP64, name
+        s.pre_jv_eval(0.0, Ud, 3.0)
+        s.matmult(Vd, out)
+        assert rel_err(out.cpu().numpy(), o.jvp(0.0, 3.0, U, V)) <= TOL_JVP, name
+
+
+@pytest.mark.parametrize("stab", ["filter", "weno"])
+def test_post_step_1d(case1d, stab, cuda):
+    name, cfg = case1d
+    cfg.apply_filter = int(stab == "filter")
+    cfg.apply_weno = int(stab == "weno")
+    cfg.shock_threshold = 0.3
+    if cfg.apply_filter and cfg.filt_cut_off == cfg.poly_deg:
+        cfg.filt_cut_off = cfg.poly_deg - 1
+    U = random_state(cfg, seed=43)
+    ref = Oracle(cfg).post_step(U)
+    with FRSolver(cfg) as s:
+        Ud = _dev(U, cuda)
+        s.apply_stabilization(Ud)
+        assert rel_err(Ud.cpu().numpy(), ref) <= TOL_FP64, name
+
+
+def test_free_stream_preserved_large(cuda):
+    """Constant state on a curved periodic mesh: R = 0 up to rounding (the
+    DoNothing problem of factory.hpp:33-56 on the sine-warped mesh)."""
+    cfg = _cfg2d(p=4, n_elems=(64, 64), box=(10.0, 10.0), geometry=A.GEOM_SINE_WARP, geom_params=(0.1, 0, 0, 0),
+                 bcs={A.LEFT: PER, A.RIGHT: PER, A.TOP: PER, A.BOTTOM: PER})
+    with FRSolver(cfg) as s:
+        U = torch.tensor([1.0, 0.5, -0.3, 2.5], dtype=torch.float64, device=cuda).repeat(s.n_dofs // 4)
+        R = torch.empty_like(U)
+        s.residual_kernel(0.0, U, R)
+        assert R.abs().max().item() < 1e-11
