@@ -191,7 +191,7 @@ def run_ours(args, ws, rank, local):
         if dist:
             dist.barrier()
 
-    wl = blast_large()
+    wl = blast_large(args.elements)
     solver = FRSolver(wl.cfg)
     U = wl.init(f"cuda:{local}")
     F = torch.empty_like(U)
@@ -282,8 +282,10 @@ def run_ours(args, ws, rank, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "elements": [1024, 1024], "poly_deg": 5, "dofs_per_rank": dofs,
-                   "state_bytes": dofs * 8, "l2": "inputs (1.21 GB) larger than L2 (126 MB); no flush",
+        "config": {"workload": WORKLOAD if args.elements == 1024 else f"{WORKLOAD} at {args.elements}^2",
+                   "elements": [args.elements, args.elements], "poly_deg": 5, "dofs_per_rank": dofs,
+                   "state_bytes": dofs * 8,
+                   "l2": f"inputs ({dofs * 8 / 1e9:.2f} GB) larger than L2 (126 MB); no flush",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
         "clocks": clk.summary(), "gpu_launches": args.steps, "roofline": roof, "e2e": e2e,
         "cpu_baseline": cpu, "bad_density_nodes": bad,
@@ -299,6 +301,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--elements", type=int, default=1024, help="elements per direction (1024 = the workload)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-all-cores", action="store_true")

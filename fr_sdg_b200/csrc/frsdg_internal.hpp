@@ -90,13 +90,22 @@ struct Fr1dArgs
 
 // Tile of elements per CTA of the 2D kernel: TX along x (contiguous in memory)
 // by TY along y, about 200-400 nodes per tile.
+// FRSDG_TX / FRSDG_TY override the shape for tuning builds.
 __host__ __device__ constexpr int tile_x(int n)
 {
+#ifdef FRSDG_TX
+    return FRSDG_TX;
+#else
     return n <= 2 ? 8 : n <= 3 ? 8 : n <= 4 ? 4 : n <= 6 ? 4 : 2;
+#endif
 }
 __host__ __device__ constexpr int tile_y(int n)
 {
+#ifdef FRSDG_TY
+    return FRSDG_TY;
+#else
     return n <= 2 ? 8 : n <= 3 ? 4 : n <= 4 ? 4 : n <= 6 ? 2 : n <= 9 ? 2 : 1;
+#endif
 }
 
 // Launchers (one translation unit per polynomial order).

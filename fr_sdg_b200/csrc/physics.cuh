@@ -159,6 +159,122 @@ __device__ __forceinline__ void riemann2(const GasParams& g, const S UL[4], cons
     Fs[3] = f3;
 }
 
+// ---- per-node records ----------------------------------------------------
+// Primitive quantities of one 2D node, computed once per node and shared by every
+// face that touches it: the reference recomputes them inside each flux and Riemann
+// call (riemann_solver.hpp:29-66, 200-225, 260-283) with the same operations.
+template <class S> struct NodePrim
+{
+    S rho_w, inv_rho, u, v, e, p, inv_covol;
+};
+
+template <int GAS, class S>
+__device__ __forceinline__ NodePrim<S> node_prim(const GasParams& g, S r0, S r1, S r2, S r3)
+{
+    NodePrim<S> q;
+    q.rho_w   = s_wrap_positive(r0);
+    q.inv_rho = s_rcp(q.rho_w);
+    q.u       = r1 * q.inv_rho;
+    q.v       = r2 * q.inv_rho;
+    const S E = s_wrap_positive(r3);
+    q.e       = E * q.inv_rho - cs<S>(0.5) * (q.u * q.u + q.v * q.v);
+    if constexpr (GAS == FRSDG_GAS_IDEAL)
+    {
+        q.inv_covol = cs<S>(1.0);
+        q.p         = (cs<S>(g.gamma) - cs<S>(1.0)) * q.rho_w * q.e;
+    }
+    else
+    {
+        q.inv_covol = s_rcp(cs<S>(1.0) - cs<S>(g.b) * q.rho_w);
+        const S cvT = q.e + cs<S>(g.a) * q.rho_w;
+        q.p = ((cs<S>(g.gamma) - cs<S>(1.0)) * q.rho_w * cvT) * q.inv_covol - cs<S>(g.a) * q.rho_w * q.rho_w;
+    }
+    return q;
+}
+
+template <int GAS, class S>
+__device__ __forceinline__ S node_sound_speed(const GasParams& g, const NodePrim<S>& q)
+{
+    if constexpr (GAS == FRSDG_GAS_IDEAL)
+        return s_sqrt(cs<S>(g.gamma) * q.p * q.inv_rho);
+    else
+    {
+        const S inv_dsq = q.inv_covol * q.inv_covol;
+        const S thermal = q.e + cs<S>(g.a) * q.rho_w;
+        const S gm1     = cs<S>(g.gamma) - cs<S>(1.0);
+        const S term1   = (cs<S>(g.gamma) * gm1 * thermal) * inv_dsq;
+        const S term2   = (gm1 * cs<S>(g.a) * q.rho_w * (cs<S>(2.0) - cs<S>(g.b) * q.rho_w)) * inv_dsq;
+        const S term3   = cs<S>(2.0) * cs<S>(g.a) * q.rho_w;
+        return s_sqrt(term1 + term2 - term3);
+    }
+}
+
+// Face record of a node: raw density and total energy, velocities, pressure and
+// sound speed -- what a Riemann solve reads from each side of a face.
+enum RecField : int
+{
+    RF_RHO = 0, RF_E = 1, RF_U = 2, RF_V = 3, RF_P = 4, RF_C = 5, RF_N = 6
+};
+
+// RiemannSolver2D (riemann_solver.hpp:189-349) on two face records.
+template <int RIEM, class S>
+__device__ __forceinline__ void riemann_rec(const S L[RF_N], const S R[RF_N], double nx_, double ny_, S Fs[4])
+{
+    using real    = typename scalar_traits<S>::real;
+    const real nx = static_cast<real>(nx_), ny = static_cast<real>(ny_);
+    const S unL = L[RF_U] * nx + L[RF_V] * ny;
+    const S utL = -L[RF_U] * ny + L[RF_V] * nx;
+    const S unR = R[RF_U] * nx + R[RF_V] * ny;
+    const S utR = -R[RF_U] * ny + R[RF_V] * nx;
+    const S cL = L[RF_C], cR = R[RF_C], pL = L[RF_P], pR = R[RF_P];
+    const S FL0 = L[RF_RHO] * unL, FL1 = L[RF_RHO] * unL * unL + pL, FL2 = L[RF_RHO] * unL * utL,
+            FL3 = (L[RF_E] + pL) * unL;
+    const S FR0 = R[RF_RHO] * unR, FR1 = R[RF_RHO] * unR * unR + pR, FR2 = R[RF_RHO] * unR * utR,
+            FR3 = (R[RF_E] + pR) * unR;
+    S f0, f1, f2, f3;
+    if constexpr (RIEM == FRSDG_RUSANOV)
+    {
+        const S smax = smooth_max(smooth_abs(unL) + cL, smooth_abs(unR) + cR);
+        const S h    = cs<S>(0.5);
+        f0 = h * (FL0 + FR0) - h * smax * (R[RF_RHO] - L[RF_RHO]);
+        f1 = h * (FL1 + FR1) - h * smax * (R[RF_RHO] * unR - L[RF_RHO] * unL);
+        f2 = h * (FL2 + FR2) - h * smax * (R[RF_RHO] * utR - L[RF_RHO] * utL);
+        f3 = h * (FL3 + FR3) - h * smax * (R[RF_E] - L[RF_E]);
+    }
+    else
+    {
+        const S sL = smooth_min(unL - cL, unR - cR);
+        const S sR = smooth_max(unL + cL, unR + cR);
+        const S rhoL_diff = L[RF_RHO] * (sL - unL);
+        const S rhoR_diff = R[RF_RHO] * (sR - unR);
+        const S sM = (pR - pL + unL * rhoL_diff - unR * rhoR_diff) * s_rcp(rhoL_diff - rhoR_diff);
+        const bool left = s_branch(sM) >= 0.0;
+        const S K0 = left ? L[RF_RHO] : R[RF_RHO];
+        const S K3 = left ? L[RF_E] : R[RF_E];
+        const S sK = left ? sL : sR;
+        const S unK = left ? unL : unR;
+        const S utK = left ? utL : utR;
+        const S pK = left ? pL : pR;
+        const S FK0 = left ? FL0 : FR0, FK1 = left ? FL1 : FR1, FK3 = left ? FL3 : FR3;
+        const S p_star = pK + K0 * (sK - unK) * (sM - unK);
+        const S inv = s_rcp(sK - sM);
+        const S st0 = (sM * (sK * K0 - FK0)) * inv;
+        const S st1 = (sM * (sK * (K0 * unK) - FK1) + sK * p_star) * inv;
+        const S st2 = utK * st0;
+        const S st3 = (sM * (sK * K3 - FK3) + sK * p_star * sM) * inv;
+        const bool takeL = s_branch(sL) >= 0.0;
+        const bool star  = left || s_branch(sR) >= 0.0;
+        f0 = takeL ? FL0 : (star ? st0 : FR0);
+        f1 = takeL ? FL1 : (star ? st1 : FR1);
+        f2 = takeL ? FL2 : (star ? st2 : FR2);
+        f3 = takeL ? FL3 : (star ? st3 : FR3);
+    }
+    Fs[0] = f0;
+    Fs[1] = f1 * nx - f2 * ny;
+    Fs[2] = f1 * ny + f2 * nx;
+    Fs[3] = f3;
+}
+
 // ---- 1D ------------------------------------------------------------------
 // make_state (riemann_solver.hpp:20-27) and euler_flux (39-46)
 template <int GAS, class S>
@@ -262,9 +378,12 @@ __device__ __forceinline__ void bc_ghost2(const BcDev& b, int dir, const GasPara
             return;
         case FRSDG_BC_WALL:
         {
-            for (int q = 0; q < 4; ++q) out[q] = in[q];
-            const int axis = dir / 2;
-            out[1 + axis]  = -in[1 + axis];
+            // the momentum component of the face axis flips (LEFT/RIGHT: x, TOP/BOTTOM: y)
+            const bool xaxis = dir < 2;
+            out[0] = in[0];
+            out[1] = xaxis ? -in[1] : in[1];
+            out[2] = xaxis ? in[2] : -in[2];
+            out[3] = in[3];
             return;
         }
         default: break;

@@ -1,19 +1,21 @@
 // residual2d.cuh -- fused FR residual of the 2D Euler equations.
 //
-// One CTA owns a tile of TX x TY elements and does, in one pass over HBM:
-//   1. load the tile's states (DMDA natural order, node-major AoS) and the four
-//      halo traces of its neighbours into shared memory (with the complex-step
-//      seed u + i h v and the prim->cons map applied on the fly when asked);
-//   2. Euler fluxes F, G of every node (euler_fluxes_2d_w_p);
-//   3. one Riemann solve per face point of the tile, on faces interior to the
-//      tile and on its four edges, with boundary ghosts on physical edges; the
-//      jumps scale*(F* - F.n) of each adjacent element go to shared memory;
-//   4. per (node, equation) the chain-rule volume term of compute_volume_term
-//      plus the four VCJH lifts, then the output form (R, -R, U_t + R or the
-//      complex-step JVP) written once, coalesced.
+// One CTA owns a tile of TX x TY elements and makes one pass over HBM:
+//   P1  every tile node: load (with the complex-step seed u + i h v or the
+//       prim->cons map applied on the fly), primitives, Euler fluxes F and G to
+//       shared memory; element-boundary nodes and the four halo traces also
+//       leave a face record (rho, rho u, rho v, rho E, u, v, p, c);
+//   P2  one Riemann solve per face point of the tile (faces inside the tile and
+//       on its edges, boundary ghosts on physical edges) giving the jumps
+//       scale*(F* - F.n) of each adjacent element, and, alongside, the
+//       eta-derivatives of each element column;
+//   P3  per element row: the xi-derivatives, the chain-rule combination, the four
+//       VCJH lifts and the requested output form, stored once.
 // Reference: PhysicsEvaluator<Traits,2>::residual_kernel and compute_volume_term,
 // include/physics_impl_2D.hpp:268-357 and 646-902, summed in the same order
 // (volume, left x-face, right x-face, bottom y-face, top y-face).
+// The derivative matrix is read from the kernel-parameter constant bank with
+// compile-time indices; tile loops have compile-time trip counts.
 #pragma once
 #include "device_math.cuh"
 #include "frsdg_internal.hpp"
@@ -22,31 +24,64 @@
 namespace frsdg
 {
 
-template <class S, int N> struct Tile2D
+__host__ __device__ constexpr int round_up32(int v) { return (v + 31) / 32 * 32; }
+
+// Block size and register cap of the 2D kernel (FRSDG_BT / FRSDG_MAXREG override
+// them for tuning builds).  A CTA's warps are spread over the SM's four
+// sub-partitions, each with a quarter of the register file, so the cap is chosen
+// for the number of co-resident CTAs wanted per SM.
+__host__ __device__ constexpr int block_threads(int n, int tile_nodes)
+{
+#ifdef FRSDG_BT
+    return FRSDG_BT;
+#else
+    return round_up32(tile_nodes > 128 ? (tile_nodes < 512 ? tile_nodes : 512) : 128);
+#endif
+}
+__host__ __device__ constexpr int reg_cap(int bt, int words)
+{
+#ifdef FRSDG_MAXREG
+    return FRSDG_MAXREG;
+#else
+    // three co-resident CTAs (one for complex): per sub-partition ceil(ctas*warps/4) warps
+    return (16384 / (32 * (((words == 2 ? 1 : 3) * (bt / 32) + 3) / 4))) / 8 * 8;
+#endif
+}
+
+template <class S, int N, int GEO> struct Tile2D
 {
     static constexpr int TX = tile_x(N);
     static constexpr int TY = tile_y(N);
     static constexpr int NN = N * N;
     static constexpr int TE = TX * TY;
-    // offsets in units of S
-    static constexpr int oU   = 0;
-    static constexpr int oHXL = oU + TE * NN * 4;
-    static constexpr int oHXR = oHXL + TY * N * 4;
-    static constexpr int oHYB = oHXR + TY * N * 4;
-    static constexpr int oHYT = oHYB + TX * N * 4;
-    static constexpr int oF   = oHYT + TX * N * 4;
+    static constexpr bool JVP = scalar_traits<S>::words == 2;
+    static constexpr int BT = block_threads(N, TE * NN);
+    static constexpr int MAXREG = reg_cap(BT, scalar_traits<S>::words) > 255 ? 255 : reg_cap(BT, scalar_traits<S>::words);
+    static constexpr int NB = 4 * N - 4;  // boundary nodes per element
+    static constexpr int NREC_E = TE * NB;
+    static constexpr int NHALO  = 2 * TY * N + 2 * TX * N;
+    static constexpr int NREC   = NREC_E + NHALO;
+    static constexpr int HXL = NREC_E, HXR = HXL + TY * N, HYB = HXR + TY * N, HYT = HYB + TX * N;
+    // shared-memory offsets in units of S
+    static constexpr int oF   = 0;
     static constexpr int oG   = oF + 4 * TE * NN;
-    static constexpr int oDXL = oG + 4 * TE * NN;
-    static constexpr int oDXR = oDXL + TE * 4 * N;
-    static constexpr int oDYB = oDXR + TE * 4 * N;
-    static constexpr int oDYT = oDYB + TE * 4 * N;
-    static constexpr int nS   = oDYT + TE * 4 * N;
-    static constexpr size_t bytes = size_t(nS) * sizeof(S) + sizeof(double) * (NN + 2 * N);
+    static constexpr int oC   = oG + 4 * TE * NN;
+    static constexpr int oRec = oC + 4 * TE * NN;
+    static constexpr int oDel = oRec + RF_N * NREC;
+    static constexpr int nS   = oDel + TE * 16 * N;
+    static constexpr size_t seed_bytes = JVP ? sizeof(double) * 4 * TE * NN : 0;
+    static constexpr size_t bytes = size_t(nS) * sizeof(S) + seed_bytes;
+    // index of boundary node (k, l) among an element's NB boundary nodes:
+    // bottom row, top row, then the interior of the left and right columns
+    __host__ __device__ static constexpr int bidx(int k, int l)
+    {
+        return l == 0 ? k : l == N - 1 ? N + k : k == 0 ? 2 * N + l - 1 : 3 * N - 2 + l - 1;
+    }
 };
 
 // Load one node's 4 values from the input vectors and form the scalar the residual
 // works on: the state itself, M(prim) for the change of variables, or the
-// complex-step point M(u + i h v).
+// complex-step point M(u + i h v) (petsc_solver_impl.hpp:288-328).
 template <class S> struct NodeLoader;
 
 template <> struct NodeLoader<double>
@@ -65,16 +100,6 @@ template <> struct NodeLoader<double>
             const double u = s[1], v = s[2];
             s[0] = rho; s[1] = rho * u; s[2] = rho * v; s[3] = rhoE;
         }
-    }
-};
-
-template <> struct NodeLoader<float>
-{
-    __device__ static void load(const Fr2dArgs& a, int64_t off, float s[4])
-    {
-        const double2 x0 = __ldg(reinterpret_cast<const double2*>(a.U + off));
-        const double2 x1 = __ldg(reinterpret_cast<const double2*>(a.U + off + 2));
-        s[0] = float(x0.x); s[1] = float(x0.y); s[2] = float(x1.x); s[3] = float(x1.y);
     }
 };
 
@@ -101,333 +126,455 @@ template <> struct NodeLoader<cplx>
     }
 };
 
-template <class S> __device__ __forceinline__ void store_out(void* out, int64_t idx, S r, const Fr2dArgs& a,
-                                                             const S& u_self);
+template <int GAS, class S>
+__device__ __forceinline__ void make_record(const GasParams& g, const S s[4], const NodePrim<S>& pr, S rec[RF_N])
+{
+    rec[RF_RHO] = s[0];
+    rec[RF_E]   = s[3];
+    rec[RF_U]   = pr.u;
+    rec[RF_V]   = pr.v;
+    rec[RF_P]   = pr.p;
+    rec[RF_C]   = node_sound_speed<GAS>(g, pr);
+}
 
-template <>
-__device__ __forceinline__ void store_out<double>(void* out, int64_t idx, double r, const Fr2dArgs& a,
-                                                  const double&)
+template <class S> struct Rec
 {
-    double v;
-    if (a.mode == MODE_RHS) v = -r;
-    else if (a.mode == MODE_IFUNC) v = __ldg(a.W + idx) + r;
-    else v = r;
-    reinterpret_cast<double*>(out)[idx] = v;
+    S v[RF_N];
+};
+
+// Boundary ghost record on a physical edge from the interior node's state (rare
+// path, kept out of line; the record returns by value).
+template <int GAS, class S>
+__device__ __noinline__ Rec<S> ghost_record(const Fr2dArgs& a, int dir, int64_t interior_off, double x, double y,
+                                            double nx, double ny)
+{
+    S s_in[4], s_out[4];
+    NodeLoader<S>::load(a, interior_off, s_in);
+    bc_ghost2<GAS>(a.bc[dir], dir, a.gas, a.t, x, y, nx, ny, a.Lx, a.Ly, s_in, s_out);
+    const NodePrim<S> pr = node_prim<GAS>(a.gas, s_out[0], s_out[1], s_out[2], s_out[3]);
+    Rec<S> out;
+    make_record<GAS>(a.gas, s_out, pr, out.v);
+    return out;
 }
-template <>
-__device__ __forceinline__ void store_out<float>(void* out, int64_t idx, float r, const Fr2dArgs& a, const float&)
+
+// One side of a face point: its record, whether it is a tile element (and which
+// element/node) or a physical-boundary ghost, and the face normal.
+template <class S> struct FaceSide
 {
-    reinterpret_cast<float*>(out)[idx] = (a.mode == MODE_RHS) ? -r : r;
+    S R[RF_N];
+    double nx, ny;
+    int e, node;     // tile element and node of this side (e < 0: halo or ghost)
+    bool bc;         // ghost from a boundary condition
+};
+
+// Locate face point t of the x-faces (XF) or y-faces of the tile, fetch both
+// side records.  Returns false (with harmless records) when t is not a face point.
+template <class S, int N, int GEO, bool XF>
+__device__ __forceinline__ bool face_prepare(const Fr2dArgs& a, bool exists, int t, int i0, int j0, int txe,
+                                             int tye, const S* sRec, FaceSide<S> sd[2])
+{
+    using T = Tile2D<S, N, GEO>;
+    constexpr int TX = T::TX, NREC = T::NREC;
+    const int pos = t % N, r = t / N;
+    int face, row, lim;
+    if constexpr (XF)
+    {
+        face = r % (TX + 1);
+        row = r / (TX + 1);
+        lim = txe;
+        exists = exists && row < tye && face <= txe;
+    }
+    else
+    {
+        row = r % TX;
+        face = r / TX;
+        lim = tye;
+        exists = exists && face <= tye && row < txe;
+    }
+    const int gI = XF ? i0 + face : i0 + row;
+    const int gJ = XF ? j0 + row : j0 + face;
+    double nx = XF ? 1.0 : 0.0, ny = XF ? 0.0 : 1.0;
+    if constexpr (GEO == GEO_CURVED)
+    {
+        if (exists)
+        {
+            const double2 nn = XF ? __ldg(reinterpret_cast<const double2*>(a.xnorm) + (int64_t(gJ) * (a.Nx + 1) + gI) * N + pos)
+                                  : __ldg(reinterpret_cast<const double2*>(a.ynorm) + (int64_t(gJ) * a.Nx + gI) * N + pos);
+            nx = nn.x;
+            ny = nn.y;
+        }
+    }
+    const bool inM = exists && face > 0, inP = exists && face < lim;
+    const bool per = XF ? a.per_x : a.per_y;
+    const int  gface = XF ? gI : gJ, gmax = XF ? a.Nx : a.Ny;
+    const bool bcM = exists && face == 0 && gface == 0 && !per;
+    const bool bcP = exists && face == lim && gface == gmax && !per;
+    const int eM = XF ? row * TX + face - 1 : (face - 1) * TX + row;
+    const int eP = XF ? row * TX + face : face * TX + row;
+    const int nodeM = XF ? pos * N + (N - 1) : (N - 1) * N + pos;
+    const int nodeP = XF ? pos * N : pos;
+    int rM = inM ? eM * T::NB + (XF ? T::bidx(N - 1, pos) : T::bidx(pos, N - 1))
+                 : (XF ? T::HXL : T::HYB) + row * N + pos;
+    int rP = inP ? eP * T::NB + (XF ? T::bidx(0, pos) : T::bidx(pos, 0))
+                 : (XF ? T::HXR : T::HYT) + row * N + pos;
+    if (!exists || bcM) rM = 0;  // any valid record keeps the arithmetic finite
+    if (!exists || bcP) rP = 0;
+#pragma unroll
+    for (int f = 0; f < RF_N; ++f)
+    {
+        sd[0].R[f] = sRec[f * NREC + rM];
+        sd[1].R[f] = sRec[f * NREC + rP];
+    }
+    sd[0].nx = sd[1].nx = nx;
+    sd[0].ny = sd[1].ny = ny;
+    sd[0].e = inM ? eM : -1;
+    sd[1].e = inP ? eP : -1;
+    sd[0].node = nodeM;
+    sd[1].node = nodeP;
+    sd[0].bc = bcM;
+    sd[1].bc = bcP;
+    // the ghost needs the global position of the face point and of its interior node
+    if (bcM) sd[0].e = -2 - (XF ? gJ * N + pos : gI * N + pos), sd[1].e = eP;
+    if (bcP) sd[1].e = -2 - (XF ? gJ * N + pos : gI * N + pos), sd[0].e = eM;
+    return exists;
 }
-template <>
-__device__ __forceinline__ void store_out<cplx>(void* out, int64_t idx, cplx r, const Fr2dArgs& a,
-                                                const cplx& u_self)
+
+// Replace the record of a boundary side by its ghost (rare path).
+template <int GAS, class S, int N, bool XF>
+__device__ __forceinline__ void face_ghost(const Fr2dArgs& a, int i0, int j0, FaceSide<S> sd[2])
 {
-    double jv = a.sigma * u_self.im * a.inv_h;
-    jv += r.im * a.inv_h;
-    reinterpret_cast<double*>(out)[idx] = jv;
+    constexpr int TX = tile_x(N), NN = N * N;
+#pragma unroll
+    for (int side = 0; side < 2; ++side)
+    {
+        if (!sd[side].bc) continue;
+        const int dir = XF ? (side == 0 ? FRSDG_LEFT : FRSDG_RIGHT) : (side == 0 ? FRSDG_BOTTOM : FRSDG_TOP);
+        const int bi = -2 - sd[side].e;
+        const double2 xy = __ldg(reinterpret_cast<const double2*>(a.bxy[dir]) + bi);
+        const FaceSide<S>& in = sd[1 - side];
+        const int64_t ioff = (int64_t(j0 + in.e / TX) * a.Nx + (i0 + in.e % TX)) * (4 * NN) + in.node * 4;
+        const Rec<S> gh = ghost_record<GAS, S>(a, dir, ioff, xy.x, xy.y, sd[side].nx, sd[side].ny);
+#pragma unroll
+        for (int f = 0; f < RF_N; ++f) sd[side].R[f] = gh.v[f];
+        sd[side].e = -1;
+    }
+}
+
+// Jumps scale*(F* - F.n) of the tile sides of a face point; F.n from the cached
+// volume fluxes (F.n = F on affine x-faces, G on affine y-faces).
+template <class S, int N, int GEO, bool XF>
+__device__ __forceinline__ void face_jumps(const Fr2dArgs& a, int i0, int j0, bool valid, const FaceSide<S> sd[2],
+                                           const S Fs[4], const S* sF, const S* sG, S* sDel)
+{
+    constexpr int TX = tile_x(N), NN = N * N;
+    if (!valid) return;
+#pragma unroll
+    for (int side = 0; side < 2; ++side)
+    {
+        const int e = sd[side].e;
+        if (e < 0) continue;
+        const int node = sd[side].node;
+        double sc;
+        if constexpr (GEO == GEO_CURVED)
+        {
+            const double* mt = a.metrics + ((int64_t(j0 + e / TX) * a.Nx + (i0 + e % TX)) * NN + node) * 4 + (XF ? 0 : 2);
+            const double2 m = __ldg(reinterpret_cast<const double2*>(mt));
+            sc = sqrt(m.x * m.x + m.y * m.y);
+        }
+        else
+            sc = XF ? a.scale_x : a.scale_y;
+        const int sdi = XF ? (side == 0 ? 1 : 0) : (side == 0 ? 3 : 2);
+        const int pos = XF ? node / N : node % N;
+#pragma unroll
+        for (int eq = 0; eq < 4; ++eq)
+        {
+            S fn;
+            if constexpr (GEO == GEO_CURVED)
+                fn = sF[(e * 4 + eq) * NN + node] * sd[side].nx + sG[(e * 4 + eq) * NN + node] * sd[side].ny;
+            else
+                fn = XF ? sF[(e * 4 + eq) * NN + node] : sG[(e * 4 + eq) * NN + node];
+            sDel[((e * 4 + sdi) * 4 + eq) * N + pos] = sc * (Fs[eq] - fn);
+        }
+    }
 }
 
 template <class S, int N, int GAS, int RIEM, int GEO>
-__global__ void __launch_bounds__(kThreads) fr2d_kernel(const Fr2dArgs a)
+__global__ void __launch_bounds__((Tile2D<S, N, GEO>::BT)) __maxnreg__((Tile2D<S, N, GEO>::MAXREG))
+fr2d_kernel(const __grid_constant__ Fr2dArgs a)
 {
-    using T = Tile2D<S, N>;
-    constexpr int TX = T::TX, TY = T::TY, NN = T::NN;
+    using T = Tile2D<S, N, GEO>;
+    constexpr int TX = T::TX, TY = T::TY, NN = T::NN, TE = T::TE, BT = T::BT, NREC = T::NREC;
+    constexpr int ND = 4 * NN;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    S*      sm  = reinterpret_cast<S*>(smem_raw);
-    double* sD  = reinterpret_cast<double*>(smem_raw + size_t(T::nS) * sizeof(S));
-    double* sdL = sD + NN;
-    double* sdR = sdL + N;
-    S* sU  = sm + T::oU;
-    S* sHXL = sm + T::oHXL;
-    S* sHXR = sm + T::oHXR;
-    S* sHYB = sm + T::oHYB;
-    S* sHYT = sm + T::oHYT;
-    S* sF  = sm + T::oF;
-    S* sG  = sm + T::oG;
-    S* sDXL = sm + T::oDXL;
-    S* sDXR = sm + T::oDXR;
-    S* sDYB = sm + T::oDYB;
-    S* sDYT = sm + T::oDYT;
+    S* sm   = reinterpret_cast<S*>(smem_raw);
+    S* sF   = sm + T::oF;
+    S* sG   = sm + T::oG;
+    S* sC   = sm + T::oC;
+    S* sRec = sm + T::oRec;
+    S* sDel = sm + T::oDel;
+    double* sSeed = reinterpret_cast<double*>(smem_raw + size_t(T::nS) * sizeof(S));
 
     const int tid = threadIdx.x;
     const int Nx = a.Nx, Ny = a.Ny;
     const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
     const int txe = min(TX, Nx - i0), tye = min(TY, Ny - j0);
-    constexpr int ND = 4 * NN; // doubles per element
+    const GasParams g = a.gas;
 
-    for (int q = tid; q < NN; q += kThreads) sD[q] = a.ops.D[q];
-    for (int q = tid; q < N; q += kThreads) { sdL[q] = a.ops.dL[q]; sdR[q] = a.ops.dR[q]; }
-
-    // ---- 1. load tile and halo traces
-    for (int q = tid; q < TY * TX * NN; q += kThreads)
+    // ---- P1: nodes of the tile; the halo traces (x-left, x-right per tile row,
+    // y-bottom, y-top per tile column) are fetched first so their latency overlaps
+    static_assert(T::NHALO <= BT, "one halo node per thread");
+    S hs[4];
+    int hrec = -1;
+    if (tid < T::NHALO)
     {
-        const int ty = q / (TX * NN), rem = q % (TX * NN), tx = rem / NN, node = rem % NN;
-        if (ty < tye && tx < txe)
-        {
-            const int64_t off = (int64_t(j0 + ty) * Nx + (i0 + tx)) * ND + node * 4;
-            S s[4];
-            NodeLoader<S>::load(a, off, s);
-            S* d = sU + ((ty * TX + tx) * NN + node) * 4;
-            d[0] = s[0]; d[1] = s[1]; d[2] = s[2]; d[3] = s[3];
-        }
-    }
-    for (int q = tid; q < 2 * TY * N + 2 * TX * N; q += kThreads)
-    {
-        int     side, r, m;
-        int     ge_i = -1, ge_j = -1, node = 0;
-        S*      dst;
+        const int q = tid;
+        int ge_i, ge_j, node, r;
+        bool ok;
         if (q < 2 * TY * N)
         {
-            side = q / (TY * N); r = (q % (TY * N)) / N; m = q % N;
-            if (r >= tye) continue;
-            ge_j = j0 + r;
-            if (side == 0) { ge_i = i0 - 1; if (ge_i < 0) { if (!a.per_x) continue; ge_i += Nx; } node = m * N + (N - 1); dst = sHXL + (r * N + m) * 4; }
-            else { ge_i = i0 + txe; if (ge_i >= Nx) { if (!a.per_x) continue; ge_i -= Nx; } node = m * N; dst = sHXR + (r * N + m) * 4; }
+            const int side = q / (TY * N), ty = (q % (TY * N)) / N, m = q % N;
+            ok = ty < tye;
+            ge_j = j0 + ty;
+            if (side == 0)
+            {
+                ge_i = i0 - 1;
+                if (ge_i < 0) { ok = ok && a.per_x; ge_i += Nx; }
+                node = m * N + (N - 1);
+                r = T::HXL + ty * N + m;
+            }
+            else
+            {
+                ge_i = i0 + txe;
+                if (ge_i >= Nx) { ok = ok && a.per_x; ge_i -= Nx; }
+                node = m * N;
+                r = T::HXR + ty * N + m;
+            }
         }
         else
         {
             const int qq = q - 2 * TY * N;
-            side = qq / (TX * N); r = (qq % (TX * N)) / N; m = qq % N;
-            if (r >= txe) continue;
-            ge_i = i0 + r;
-            if (side == 0) { ge_j = j0 - 1; if (ge_j < 0) { if (!a.per_y) continue; ge_j += Ny; } node = (N - 1) * N + m; dst = sHYB + (r * N + m) * 4; }
-            else { ge_j = j0 + tye; if (ge_j >= Ny) { if (!a.per_y) continue; ge_j -= Ny; } node = m; dst = sHYT + (r * N + m) * 4; }
+            const int side = qq / (TX * N), tx = (qq % (TX * N)) / N, m = qq % N;
+            ok = tx < txe;
+            ge_i = i0 + tx;
+            if (side == 0)
+            {
+                ge_j = j0 - 1;
+                if (ge_j < 0) { ok = ok && a.per_y; ge_j += Ny; }
+                node = (N - 1) * N + m;
+                r = T::HYB + tx * N + m;
+            }
+            else
+            {
+                ge_j = j0 + tye;
+                if (ge_j >= Ny) { ok = ok && a.per_y; ge_j -= Ny; }
+                node = m;
+                r = T::HYT + tx * N + m;
+            }
         }
-        const int64_t off = (int64_t(ge_j) * Nx + ge_i) * ND + node * 4;
-        S s[4];
-        NodeLoader<S>::load(a, off, s);
-        dst[0] = s[0]; dst[1] = s[1]; dst[2] = s[2]; dst[3] = s[3];
-    }
-    __syncthreads();
-
-    // ---- 2. volume fluxes
-    const GasParams g = a.gas;
-    for (int q = tid; q < TY * TX * NN; q += kThreads)
-    {
-        const int e = q / NN, node = q % NN;
-        const int ty = e / TX, tx = e % TX;
-        if (ty < tye && tx < txe)
+        if (ok)
         {
-            const S* u = sU + q * 4;
-            S s[4] = {u[0], u[1], u[2], u[3]};
+            NodeLoader<S>::load(a, (int64_t(ge_j) * Nx + ge_i) * ND + node * 4, hs);
+            hrec = r;
+        }
+    }
+    for (int q = tid; q < TE * NN; q += BT)
+    {
+        const int e = q / NN, node = q % NN, tx = e % TX, ty = e / TX, k = node % N, l = node / N;
+        if (tx < txe && ty < tye)
+        {
+            const int64_t off = (int64_t(j0 + ty) * Nx + (i0 + tx)) * ND + node * 4;
+            S s[4];
+            NodeLoader<S>::load(a, off, s);
+            if constexpr (T::JVP)
+            {
+#pragma unroll
+                for (int eq = 0; eq < 4; ++eq) sSeed[(e * 4 + eq) * NN + node] = s_im(s[eq]);
+            }
             if (!(s_re(s[0]) > 0.0) && a.bad) atomicAdd(a.bad, 1ull);
-            const Prim2<S> pr = prim2<GAS>(g, s);
-            S F[4], G[4];
-            fluxes2(s, pr, F, G);
-#pragma unroll
-            for (int eq = 0; eq < 4; ++eq)
+            const NodePrim<S> pr = node_prim<GAS>(g, s[0], s[1], s[2], s[3]);
+            const S rEp = s[3] + pr.p;
+            const S ruv = s[1] * pr.v;
+            S* f = sF + e * 4 * NN + node;
+            S* gg = sG + e * 4 * NN + node;
+            f[0 * NN] = s[1];
+            f[1 * NN] = s[1] * pr.u + pr.p;
+            f[2 * NN] = ruv;
+            f[3 * NN] = pr.u * rEp;
+            gg[0 * NN] = s[2];
+            gg[1 * NN] = ruv;
+            gg[2 * NN] = s[2] * pr.v + pr.p;
+            gg[3 * NN] = pr.v * rEp;
+            if (k == 0 || k == N - 1 || l == 0 || l == N - 1)
             {
-                sF[(eq * T::TE + e) * NN + node] = F[eq];
-                sG[(eq * T::TE + e) * NN + node] = G[eq];
+                S rec[RF_N];
+                make_record<GAS>(g, s, pr, rec);
+                const int r = e * T::NB + T::bidx(k, l);
+#pragma unroll
+                for (int fld = 0; fld < RF_N; ++fld) sRec[fld * NREC + r] = rec[fld];
             }
         }
     }
+    if (hrec >= 0)
+    {
+        const NodePrim<S> pr = node_prim<GAS>(g, hs[0], hs[1], hs[2], hs[3]);
+        S rec[RF_N];
+        make_record<GAS>(g, hs, pr, rec);
+#pragma unroll
+        for (int fld = 0; fld < RF_N; ++fld) sRec[fld * NREC + hrec] = rec[fld];
+    }
     __syncthreads();
 
-    // ---- 3. faces
-    const int nxf = (txe + 1) * tye * N;
-    const int nyf = txe * (tye + 1) * N;
-    for (int q = tid; q < nxf + nyf; q += kThreads)
+    // ---- P2: face points and element columns.  Each face thread solves one x-face
+    // point and one y-face point (two independent Riemann problems in flight).
+    constexpr int NXF = (TX + 1) * TY * N, NYF = TX * (TY + 1) * N, NCOL = TE * 4 * N;
+    constexpr int NFP = NXF > NYF ? NXF : NYF;
+    constexpr int PFP = round_up32(NFP), PCOL = round_up32(NCOL);
+    for (int t = tid; t < PFP + PCOL; t += BT)
     {
-        S UA[4], UB[4];
-        double nx, ny;
-        if (q < nxf)
+        if (t < PFP)
         {
-            // x-face I (0..txe) of tile row ty, face point l
-            const int l = q % N, r = q / N, I = r % (txe + 1), ty = r / (txe + 1);
-            const int gI = i0 + I, gj = j0 + ty;
-            if constexpr (GEO == GEO_CURVED)
-            {
-                const double2 nn = __ldg(reinterpret_cast<const double2*>(a.xnorm) + (int64_t(gj) * (Nx + 1) + gI) * N + l);
-                nx = nn.x; ny = nn.y;
-            }
-            else { nx = 1.0; ny = 0.0; }
-            const bool inL = I > 0, inR = I < txe;
-            const bool bcL = !inL && gI == 0 && !a.per_x;
-            const bool bcR = !inR && gI == Nx && !a.per_x;
-            const S* pL = inL ? sU + ((ty * TX + I - 1) * NN + l * N + (N - 1)) * 4 : sHXL + (ty * N + l) * 4;
-            const S* pR = inR ? sU + ((ty * TX + I) * NN + l * N) * 4 : sHXR + (ty * N + l) * 4;
-            if (!bcL) { UA[0] = pL[0]; UA[1] = pL[1]; UA[2] = pL[2]; UA[3] = pL[3]; }
-            if (!bcR) { UB[0] = pR[0]; UB[1] = pR[1]; UB[2] = pR[2]; UB[3] = pR[3]; }
-            if (bcL)
-            {
-                const double2 xy = __ldg(reinterpret_cast<const double2*>(a.bxy[FRSDG_LEFT]) + gj * N + l);
-                bc_ghost2<GAS>(a.bc[FRSDG_LEFT], FRSDG_LEFT, g, a.t, xy.x, xy.y, nx, ny, a.Lx, a.Ly, UB, UA);
-            }
-            if (bcR)
-            {
-                const double2 xy = __ldg(reinterpret_cast<const double2*>(a.bxy[FRSDG_RIGHT]) + gj * N + l);
-                bc_ghost2<GAS>(a.bc[FRSDG_RIGHT], FRSDG_RIGHT, g, a.t, xy.x, xy.y, nx, ny, a.Lx, a.Ly, UA, UB);
-            }
-            S Fs[4];
-            riemann2<RIEM, GAS>(g, UA, UB, nx, ny, Fs);
-            if (inL)
-            {
-                const int e = ty * TX + I - 1, node = l * N + (N - 1);
-                double sc;
-                if constexpr (GEO == GEO_CURVED)
-                {
-                    const double2 m = __ldg(reinterpret_cast<const double2*>(a.metrics + ((int64_t(gj) * Nx + gI - 1) * NN + node) * 4));
-                    sc = sqrt(m.x * m.x + m.y * m.y);
-                }
-                else sc = a.scale_x;
-#pragma unroll
-                for (int eq = 0; eq < 4; ++eq)
-                {
-                    const S fn = sF[(eq * T::TE + e) * NN + node] * nx + sG[(eq * T::TE + e) * NN + node] * ny;
-                    sDXR[(e * 4 + eq) * N + l] = sc * (Fs[eq] - fn);
-                }
-            }
-            if (inR)
-            {
-                const int e = ty * TX + I, node = l * N;
-                double sc;
-                if constexpr (GEO == GEO_CURVED)
-                {
-                    const double2 m = __ldg(reinterpret_cast<const double2*>(a.metrics + ((int64_t(gj) * Nx + gI) * NN + node) * 4));
-                    sc = sqrt(m.x * m.x + m.y * m.y);
-                }
-                else sc = a.scale_x;
-#pragma unroll
-                for (int eq = 0; eq < 4; ++eq)
-                {
-                    const S fn = sF[(eq * T::TE + e) * NN + node] * nx + sG[(eq * T::TE + e) * NN + node] * ny;
-                    sDXL[(e * 4 + eq) * N + l] = sc * (Fs[eq] - fn);
-                }
-            }
+            FaceSide<S> xs[2], ys[2];
+            const bool vx = face_prepare<S, N, GEO, true>(a, t < NXF, t, i0, j0, txe, tye, sRec, xs);
+            const bool vy = face_prepare<S, N, GEO, false>(a, t < NYF, t, i0, j0, txe, tye, sRec, ys);
+            if (!vx && !vy) continue;
+            if (xs[0].bc || xs[1].bc) face_ghost<GAS, S, N, true>(a, i0, j0, xs);
+            if (ys[0].bc || ys[1].bc) face_ghost<GAS, S, N, false>(a, i0, j0, ys);
+            S Fx[4], Fy[4];
+            riemann_rec<RIEM>(xs[0].R, xs[1].R, xs[0].nx, xs[0].ny, Fx);
+            riemann_rec<RIEM>(ys[0].R, ys[1].R, ys[0].nx, ys[0].ny, Fy);
+            face_jumps<S, N, GEO, true>(a, i0, j0, vx, xs, Fx, sF, sG, sDel);
+            face_jumps<S, N, GEO, false>(a, i0, j0, vy, ys, Fy, sF, sG, sDel);
         }
         else
         {
-            // y-face J (0..tye) of tile column tx, face point k
-            const int qq = q - nxf;
-            const int k = qq % N, r = qq / N, tx = r % txe, J = r / txe;
-            const int gi = i0 + tx, gJ = j0 + J;
+            // column (e, eq, k): eta-derivatives of G (and of F on curved meshes)
+            const int tt = t - PFP;
+            if (tt >= NCOL) continue;
+            const int k = tt % N, r = tt / N, eq = r % 4, e = r / 4;
+            if ((e % TX) >= txe || (e / TX) >= tye) continue;
+            const S* Gc = sG + (e * 4 + eq) * NN + k;
+            S gv[N];
+#pragma unroll
+            for (int m = 0; m < N; ++m) gv[m] = Gc[m * N];
             if constexpr (GEO == GEO_CURVED)
             {
-                const double2 nn = __ldg(reinterpret_cast<const double2*>(a.ynorm) + (int64_t(gJ) * Nx + gi) * N + k);
-                nx = nn.x; ny = nn.y;
-            }
-            else { nx = 0.0; ny = 1.0; }
-            const bool inB = J > 0, inT = J < tye;
-            const bool bcB = !inB && gJ == 0 && !a.per_y;
-            const bool bcT = !inT && gJ == Ny && !a.per_y;
-            const S* pB = inB ? sU + (((J - 1) * TX + tx) * NN + (N - 1) * N + k) * 4 : sHYB + (tx * N + k) * 4;
-            const S* pT = inT ? sU + ((J * TX + tx) * NN + k) * 4 : sHYT + (tx * N + k) * 4;
-            if (!bcB) { UA[0] = pB[0]; UA[1] = pB[1]; UA[2] = pB[2]; UA[3] = pB[3]; }
-            if (!bcT) { UB[0] = pT[0]; UB[1] = pT[1]; UB[2] = pT[2]; UB[3] = pT[3]; }
-            if (bcB)
-            {
-                const double2 xy = __ldg(reinterpret_cast<const double2*>(a.bxy[FRSDG_BOTTOM]) + gi * N + k);
-                bc_ghost2<GAS>(a.bc[FRSDG_BOTTOM], FRSDG_BOTTOM, g, a.t, xy.x, xy.y, nx, ny, a.Lx, a.Ly, UB, UA);
-            }
-            if (bcT)
-            {
-                const double2 xy = __ldg(reinterpret_cast<const double2*>(a.bxy[FRSDG_TOP]) + gi * N + k);
-                bc_ghost2<GAS>(a.bc[FRSDG_TOP], FRSDG_TOP, g, a.t, xy.x, xy.y, nx, ny, a.Lx, a.Ly, UA, UB);
-            }
-            S Fs[4];
-            riemann2<RIEM, GAS>(g, UA, UB, nx, ny, Fs);
-            if (inB)
-            {
-                const int e = (J - 1) * TX + tx, node = (N - 1) * N + k;
-                double sc;
-                if constexpr (GEO == GEO_CURVED)
-                {
-                    const double2 m = __ldg(reinterpret_cast<const double2*>(a.metrics + ((int64_t(gJ - 1) * Nx + gi) * NN + node) * 4) + 1);
-                    sc = sqrt(m.x * m.x + m.y * m.y);
-                }
-                else sc = a.scale_y;
+                const S* Fc = sF + (e * 4 + eq) * NN + k;
+                S fv[N];
 #pragma unroll
-                for (int eq = 0; eq < 4; ++eq)
+                for (int m = 0; m < N; ++m) fv[m] = Fc[m * N];
+                const double* mt = a.metrics + ((int64_t(j0 + e / TX) * Nx + (i0 + e % TX)) * NN + k) * 4 + 2;
+#pragma unroll
+                for (int l = 0; l < N; ++l)
                 {
-                    const S fn = sF[(eq * T::TE + e) * NN + node] * nx + sG[(eq * T::TE + e) * NN + node] * ny;
-                    sDYT[(e * 4 + eq) * N + k] = sc * (Fs[eq] - fn);
+                    S dG = S(0.0), dF = S(0.0);
+#pragma unroll
+                    for (int m = 0; m < N; ++m)
+                    {
+                        dG = dG + a.ops.D[l * N + m] * gv[m];
+                        dF = dF + a.ops.D[l * N + m] * fv[m];
+                    }
+                    const double2 me = __ldg(reinterpret_cast<const double2*>(mt + l * N * 4));
+                    sC[(e * 4 + eq) * NN + l * N + k] = me.x * dF + me.y * dG;
                 }
             }
-            if (inT)
+            else
             {
-                const int e = J * TX + tx, node = k;
-                double sc;
-                if constexpr (GEO == GEO_CURVED)
-                {
-                    const double2 m = __ldg(reinterpret_cast<const double2*>(a.metrics + ((int64_t(gJ) * Nx + gi) * NN + node) * 4) + 1);
-                    sc = sqrt(m.x * m.x + m.y * m.y);
-                }
-                else sc = a.scale_y;
 #pragma unroll
-                for (int eq = 0; eq < 4; ++eq)
+                for (int l = 0; l < N; ++l)
                 {
-                    const S fn = sF[(eq * T::TE + e) * NN + node] * nx + sG[(eq * T::TE + e) * NN + node] * ny;
-                    sDYB[(e * 4 + eq) * N + k] = sc * (Fs[eq] - fn);
+                    S dG = S(0.0);
+#pragma unroll
+                    for (int m = 0; m < N; ++m) dG = dG + a.ops.D[l * N + m] * gv[m];
+                    sC[(e * 4 + eq) * NN + l * N + k] = a.eta_y * dG;
                 }
             }
         }
     }
     __syncthreads();
 
-    // ---- 4. volume term + lifts, output
-    for (int q = tid; q < TY * TX * ND; q += kThreads)
+    // ---- P3: element rows (e, eq, l), equation fastest across lanes
+    for (int t = tid; t < TE * 4 * N; t += BT)
     {
-        const int e = q / ND, rem = q % ND, node = rem >> 2, eq = rem & 3;
-        const int ty = e / TX, tx = e % TX;
-        if (ty >= tye || tx >= txe) continue;
-        const int k = node % N, l = node / N;
-        const S* Fe = sF + (eq * T::TE + e) * NN;
-        const S* Ge = sG + (eq * T::TE + e) * NN;
-        S dF_dxi = S(0.0), dG_deta = S(0.0);
-        S dG_dxi = S(0.0), dF_deta = S(0.0);
+        const int eq = t % 4, l = (t / 4) % N, e = t / (4 * N);
+        const int tx = e % TX, ty = e / TX;
+        if (tx >= txe || ty >= tye) continue;
+        const S* Fr = sF + (e * 4 + eq) * NN + l * N;
+        S fv[N];
 #pragma unroll
-        for (int m = 0; m < N; ++m)
-        {
-            if constexpr (GEO == GEO_CURVED) dG_dxi = dG_dxi + sD[k * N + m] * Ge[l * N + m];
-            dF_dxi = dF_dxi + sD[k * N + m] * Fe[l * N + m];
-        }
-#pragma unroll
-        for (int m = 0; m < N; ++m)
-        {
-            dG_deta = dG_deta + sD[l * N + m] * Ge[m * N + k];
-            if constexpr (GEO == GEO_CURVED) dF_deta = dF_deta + sD[l * N + m] * Fe[m * N + k];
-        }
-        const int64_t gidx = (int64_t(j0 + ty) * Nx + (i0 + tx)) * ND + rem;
-        S R;
+        for (int m = 0; m < N; ++m) fv[m] = Fr[m];
+        const double dLl = a.ops.dL[l], dRl = a.ops.dR[l];
+        const S dxl = sDel[((e * 4 + 0) * 4 + eq) * N + l];
+        const S dxr = sDel[((e * 4 + 1) * 4 + eq) * N + l];
+        const S* dyb = sDel + ((e * 4 + 2) * 4 + eq) * N;
+        const S* dyt = sDel + ((e * 4 + 3) * 4 + eq) * N;
+        const int64_t gbase = (int64_t(j0 + ty) * Nx + (i0 + tx)) * ND + eq;
+        S gr[N];
         if constexpr (GEO == GEO_CURVED)
         {
-            const double* mt = a.metrics + (int64_t(j0 + ty) * Nx + (i0 + tx)) * ND + node * 4;
-            const double2 m0 = __ldg(reinterpret_cast<const double2*>(mt));
-            const double2 m1 = __ldg(reinterpret_cast<const double2*>(mt) + 1);
-            const S px = m0.x * dF_dxi + m1.x * dF_deta;
-            const S py = m0.y * dG_dxi + m1.y * dG_deta;
-            R = px + py;
+            const S* Gr = sG + (e * 4 + eq) * NN + l * N;
+#pragma unroll
+            for (int m = 0; m < N; ++m) gr[m] = Gr[m];
         }
-        else
+#pragma unroll
+        for (int k = 0; k < N; ++k)
         {
-            const S px = a.xi_x * dF_dxi;
-            const S py = a.eta_y * dG_deta;
-            R = px + py;
+            S dF = S(0.0);
+#pragma unroll
+            for (int m = 0; m < N; ++m) dF = dF + a.ops.D[k * N + m] * fv[m];
+            S R;
+            if constexpr (GEO == GEO_CURVED)
+            {
+                S dG = S(0.0);
+#pragma unroll
+                for (int m = 0; m < N; ++m) dG = dG + a.ops.D[k * N + m] * gr[m];
+                const double2 mx = __ldg(reinterpret_cast<const double2*>(
+                    a.metrics + ((int64_t(j0 + ty) * Nx + (i0 + tx)) * NN + l * N + k) * 4));
+                R = (mx.x * dF + mx.y * dG) + sC[(e * 4 + eq) * NN + l * N + k];
+            }
+            else
+            {
+                const S px = a.xi_x * dF;
+                R = px + sC[(e * 4 + eq) * NN + l * N + k];
+            }
+            R = R + dxl * a.ops.dL[k];
+            R = R + dxr * a.ops.dR[k];
+            R = R + dyb[k] * dLl;
+            R = R + dyt[k] * dRl;
+            const int64_t gidx = gbase + (l * N + k) * 4;
+            double* out = reinterpret_cast<double*>(a.out);
+            if constexpr (T::JVP)
+            {
+                double jv = a.sigma * sSeed[(e * 4 + eq) * NN + l * N + k] * a.inv_h;
+                jv += s_im(R) * a.inv_h;
+                out[gidx] = jv;
+            }
+            else
+            {
+                const double r = s_re(R);
+                if (a.mode == MODE_RHS) out[gidx] = -r;
+                else if (a.mode == MODE_IFUNC) out[gidx] = __ldg(a.W + gidx) + r;
+                else out[gidx] = r;
+            }
         }
-        R = R + sDXL[(e * 4 + eq) * N + l] * sdL[k];
-        R = R + sDXR[(e * 4 + eq) * N + l] * sdR[k];
-        R = R + sDYB[(e * 4 + eq) * N + k] * sdL[l];
-        R = R + sDYT[(e * 4 + eq) * N + k] * sdR[l];
-        store_out<S>(a.out, gidx, R, a, sU[(e * NN + node) * 4 + eq]);
     }
 }
 
 template <class S, int N, int GAS, int RIEM, int GEO>
 cudaError_t launch_fr2d_kernel(const Fr2dArgs& a, cudaStream_t st)
 {
-    using T = Tile2D<S, N>;
+    using T = Tile2D<S, N, GEO>;
     auto kern = fr2d_kernel<S, N, GAS, RIEM, GEO>;
     static bool attr_done = false;
     if (!attr_done)
     {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(T::bytes));
         if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e != cudaSuccess) return e;
         attr_done = true;
     }
     dim3 grid((a.Nx + T::TX - 1) / T::TX, (a.Ny + T::TY - 1) / T::TY);
-    kern<<<grid, kThreads, T::bytes, st>>>(a);
+    kern<<<grid, T::BT, T::bytes, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -7,8 +7,12 @@ from fr_sdg_b200 import _abi as A
 
 # Tolerance of the FP64 GPU path against the oracle: max|gpu - oracle| / max|oracle|.
 TOL_FP64 = 1e-12
-# Complex-step JVP: Im(R(u + i h v)) / h carries the rounding of R's imaginary part.
-TOL_JVP = 1e-11
+# Complex-step JVP.  Where a slip wall or a symmetric state makes the two wave
+# speeds of smooth_max tie, the argument of smooth_abs is rounding noise x ~ 1e-16
+# and its derivative x / sqrt(x^2 + 1e-14) ~ x / 1e-7 amplifies that noise by 1e7
+# (macro_and_libc.hpp:80-102), so two correct implementations differ there at the
+# 1e-11 level; elsewhere they agree to ~1e-15.
+TOL_JVP = 1e-10
 
 
 def rel_err(got, ref) -> float:
