@@ -34,16 +34,18 @@ FRSDG_DECL_ALL(cplx)
 
 namespace
 {
-thread_local std::string g_err;
+// Last error of the calling thread, in a fixed buffer so that reporting an error
+// never allocates.
+thread_local char g_err[256];
 
-int fail(int code, const std::string& msg)
+int fail(int code, const char* msg)
 {
-    g_err = msg;
+    std::snprintf(g_err, sizeof(g_err), "%s", msg);
     return code;
 }
 int cuda_fail(cudaError_t e, const char* what)
 {
-    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    std::snprintf(g_err, sizeof(g_err), "%s: %s", what, cudaGetErrorString(e));
     return FRSDG_ERR_CUDA;
 }
 
@@ -82,7 +84,12 @@ template <class S> cudaError_t dispatch1d(int n, int gas, int riem, const Fr1dAr
 
 bool is_native_bc(int k) { return k == FRSDG_BC_OUTFLOW || k == FRSDG_BC_WALL || k == FRSDG_BC_PERIODIC; }
 
-int validate(const frsdg_config& c)
+} // namespace
+
+namespace frsdg
+{
+// Configuration checks shared by frsdg_create and the allocation-free entry point.
+int validate_config(const frsdg_config& c)
 {
     if (c.dim != 1 && c.dim != 2) return fail(FRSDG_ERR_ARG, "dim must be 1 or 2");
     if (c.poly_deg < 1 || c.poly_deg > 9) return fail(FRSDG_ERR_ARG, "poly_deg must be in [1, 9]");
@@ -114,7 +121,9 @@ int validate(const frsdg_config& c)
     return FRSDG_OK;
 }
 
-} // namespace
+int report(int code, const char* msg) { return fail(code, msg); }
+int report_cuda(cudaError_t e, const char* what) { return cuda_fail(e, what); }
+} // namespace frsdg
 
 struct frsdg_handle
 {
@@ -167,7 +176,7 @@ template <class T> static int upload(T** dst, const std::vector<T>& v)
 extern "C" {
 
 int frsdg_abi_version(void) { return FRSDG_ABI_VERSION; }
-const char* frsdg_last_error(void) { return g_err.c_str(); }
+const char* frsdg_last_error(void) { return g_err; }
 
 int frsdg_config_default(frsdg_config* c)
 {
@@ -238,7 +247,7 @@ int frsdg_create(const frsdg_config* cfg, frsdg_handle** out)
 {
     if (!cfg || !out) return fail(FRSDG_ERR_ARG, "null argument");
     *out = nullptr;
-    int rc = validate(*cfg);
+    int rc = validate_config(*cfg);
     if (rc) return rc;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)

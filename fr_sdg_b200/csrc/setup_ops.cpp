@@ -48,17 +48,13 @@ double legendre_dp(int k, double x)
 }
 } // namespace
 
-RefElem build_ref_element(int p, double c)
+void ref_element_into(int p, double c, double* X, double* W, double* Dm, double* DL, double* DR)
 {
     if (p < 1 || p > 9) throw std::invalid_argument("poly_deg must be in [1, 9]");
-    RefElem r;
-    r.p = p;
-    r.n = p + 1;
-    const int n = r.n;
-    r.x.assign(n, 0.0);
-    r.w.assign(n, 0.0);
-    r.x[0] = -1.0;
-    r.x[p] = 1.0;
+    const int n = p + 1;
+    for (int k = 0; k < n; ++k) X[k] = W[k] = 0.0;
+    X[0] = -1.0;
+    X[p] = 1.0;
     const double pi = 3.14159265358979323846;
     for (int j = 1; j <= (n + 1) / 2 - 1; ++j)
     {
@@ -73,31 +69,33 @@ RefElem build_ref_element(int p, double c)
             x += dx;
             if (std::fabs(dx) <= 4.0 * std::numeric_limits<double>::epsilon() * std::fabs(x)) break;
         }
-        r.x[j]     = x;
-        r.x[p - j] = -x;
+        X[j]     = x;
+        X[p - j] = -x;
     }
-    if (p % 2 == 0) r.x[p / 2] = 0.0;
+    if (p % 2 == 0) X[p / 2] = 0.0;
     for (int k = 0; k < n; ++k)
     {
-        const double Pp = legendre_p(p, r.x[k]);
-        r.w[k]          = 2.0 / (double(p) * (p + 1) * Pp * Pp);
+        const double Pp = legendre_p(p, X[k]);
+        W[k]            = 2.0 / (double(p) * (p + 1) * Pp * Pp);
     }
     // differentiation matrix
-    r.D.assign(n * n, 0.0);
-    std::vector<double> a(n, 1.0);
+    double a[16];
     for (int i = 0; i < n; ++i)
+    {
+        a[i] = 1.0;
         for (int k = 0; k < n; ++k)
-            if (k != i) a[i] *= r.x[i] - r.x[k];
+            if (k != i) a[i] *= X[i] - X[k];
+    }
     for (int i = 0; i < n; ++i)
         for (int j = 0; j < n; ++j)
         {
-            if (i != j) r.D[i * n + j] = a[i] / (a[j] * (r.x[i] - r.x[j]));
+            if (i != j) Dm[i * n + j] = a[i] / (a[j] * (X[i] - X[j]));
             else
             {
-                double s = 0.0;
+                double sum = 0.0;
                 for (int k = 0; k < n; ++k)
-                    if (k != i) s += 1.0 / (r.x[i] - r.x[k]);
-                r.D[i * n + i] = s;
+                    if (k != i) sum += 1.0 / (X[i] - X[k]);
+                Dm[i * n + i] = sum;
             }
         }
     // VCJH: eta_p = c (2p+1) (a_p p!)^2 / 2 with a_p = (2p)! / (2^p (p!)^2)
@@ -108,24 +106,36 @@ RefElem build_ref_element(int p, double c)
     const double apf  = ap * pf;
     const double eta  = c * double(2 * p + 1) * apf * apf / 2.0;
     const double sign = (p % 2 == 0) ? 1.0 : -1.0;
-    r.dL.assign(n, 0.0);
-    r.dR.assign(n, 0.0);
     for (int i = 0; i < n; ++i)
     {
-        const double d0 = legendre_dp(p, r.x[i]);
-        const double dm = legendre_dp(p - 1, r.x[i]);
-        const double dp = legendre_dp(p + 1, r.x[i]);
+        const double d0 = legendre_dp(p, X[i]);
+        const double dm = legendre_dp(p - 1, X[i]);
+        const double dp = legendre_dp(p + 1, X[i]);
         const double t  = (eta * dm + dp) / (1.0 + eta);
-        r.dL[i] = sign * 0.5 * (d0 - t);
-        r.dR[i] = 0.5 * (d0 + t);
+        DL[i] = sign * 0.5 * (d0 - t);
+        DR[i] = 0.5 * (d0 + t);
     }
+}
+
+RefElem build_ref_element(int p, double c)
+{
+    if (p < 1 || p > 9) throw std::invalid_argument("poly_deg must be in [1, 9]");
+    RefElem r;
+    r.p = p;
+    r.n = p + 1;
+    r.x.assign(r.n, 0.0);
+    r.w.assign(r.n, 0.0);
+    r.D.assign(r.n * r.n, 0.0);
+    r.dL.assign(r.n, 0.0);
+    r.dR.assign(r.n, 0.0);
+    ref_element_into(p, c, r.x.data(), r.w.data(), r.D.data(), r.dL.data(), r.dR.data());
     return r;
 }
 
-std::vector<double> build_filter_matrix(const RefElem& re, int nc, int s, double alpha)
+void filter_matrix_into(int p, const double* X, const double* W, int nc, int s, double alpha, double* F)
 {
-    const int n = re.n, p = re.p;
-    std::vector<double> sigma(n), gam(n), V(n * n);
+    const int n = p + 1;
+    double sigma[16], gam[16], V[16 * 16];
     for (int i = 0; i < n; ++i)
     {
         if (i < nc) sigma[i] = 1.0;
@@ -137,15 +147,20 @@ std::vector<double> build_filter_matrix(const RefElem& re, int nc, int s, double
         gam[i] = (i < p) ? 2.0 / (2.0 * i + 1.0) : 2.0 / double(p);
     }
     for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j) V[i * n + j] = legendre_p(j, re.x[i]);
-    std::vector<double> F(n * n, 0.0);
+        for (int j = 0; j < n; ++j) V[i * n + j] = legendre_p(j, X[i]);
     for (int i = 0; i < n; ++i)
         for (int k = 0; k < n; ++k)
         {
             double acc = 0.0;
-            for (int j = 0; j < n; ++j) acc += V[i * n + j] * sigma[j] * re.w[k] * V[k * n + j] / gam[j];
+            for (int j = 0; j < n; ++j) acc += V[i * n + j] * sigma[j] * W[k] * V[k * n + j] / gam[j];
             F[i * n + k] = acc;
         }
+}
+
+std::vector<double> build_filter_matrix(const RefElem& re, int nc, int s, double alpha)
+{
+    std::vector<double> F(re.n * re.n, 0.0);
+    filter_matrix_into(re.p, re.x.data(), re.w.data(), nc, s, alpha, F.data());
     return F;
 }
 

@@ -21,6 +21,12 @@ RefElem build_ref_element(int p, double radau_corr);
 // Spectral filter matrix V diag(sigma) V^-1, row-major n*n.
 std::vector<double> build_filter_matrix(const RefElem& re, int cut_off, int strength, double alpha);
 
+// Heap-free forms of the two builders above, writing into caller arrays of at
+// least n (and n*n for D and F) entries, n = p + 1 <= 10.
+void ref_element_into(int p, double radau_corr, double* x, double* w, double* D, double* dL, double* dR);
+void filter_matrix_into(int p, const double* x, const double* w, int cut_off, int strength, double alpha,
+                        double* F);
+
 struct GeomJacobian
 {
     double dx_dcsi, dy_dcsi, dx_deta, dy_deta;

@@ -183,8 +183,9 @@ int frsdg_rhs_host(frsdg_handle* h, double t, const double* U_host, double* rhs_
                    void* stream);
 
 /* Device-side health word: number of nodes seen with a non-positive or
- * non-finite density by the last residual call (0 = healthy).  Synchronises the
- * handle's last stream. */
+ * non-finite density by the residual calls since the previous frsdg_status call
+ * (0 = healthy); the count restarts at zero.  Synchronises the handle's last
+ * stream. */
 int frsdg_status(frsdg_handle* h, int64_t* bad_nodes);
 
 /* Host-only set-up operators, usable without a GPU.
