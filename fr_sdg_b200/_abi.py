@@ -12,6 +12,8 @@ from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "libfrsdg.so"
 
+POST_STEP_STATIC_MAX_DOFS = 4194304  # FRSDG_POST_STEP_STATIC_MAX_DOFS in include/frsdg.h
+
 # status codes
 OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NODEVICE = 0, -1, -2, -3, -4, -5
 # policies
@@ -64,6 +66,7 @@ SIGNATURES = {
     "frsdg_jvp_prepare": (C.c_int, [_P, _D, _D, _P]),
     "frsdg_jvp": (C.c_int, [_P, _P, _P, _P]),
     "frsdg_post_step": (C.c_int, [_P, _P, _P]),
+    "frsdg_post_step_static": (C.c_int, [C.POINTER(frsdg_config), _P, _P]),
     "frsdg_prim_to_cons": (C.c_int, [_P, _P, _P, _P]),
     "frsdg_rhs_host": (C.c_int, [_P, _D, _P, _P, _P]),
     "frsdg_status": (C.c_int, [_P, C.POINTER(C.c_int64)]),

@@ -188,6 +188,23 @@ int frsdg_rhs_host(frsdg_handle* h, double t, const double* U_host, double* rhs_
  * stream. */
 int frsdg_status(frsdg_handle* h, int64_t* bad_nodes);
 
+/* Largest solution (in doubles) frsdg_post_step_static accepts: 4,194,304 (32 MiB
+ * of scratch held on every device that loads the library). */
+#define FRSDG_POST_STEP_STATIC_MAX_DOFS 4194304
+
+/* frsdg_post_step for callers that must not allocate device memory (for example
+ * while a CUDA stream is being captured into a graph, where cudaMalloc is not
+ * allowed, or under a memory manager that owns every allocation).  It has no
+ * counterpart in the reference.  It takes the configuration instead of a handle
+ * and allocates nothing: the copy the WENO limiter reads from is a fixed device
+ * array of FRSDG_POST_STEP_STATIC_MAX_DOFS doubles inside the library; larger
+ * solutions are rejected with FRSDG_ERR_ARG.  The first call on each device looks
+ * up that array's device address, so make the first call outside any stream
+ * capture.  Calls share the array: calls that overlap on the GPU (different
+ * streams, or different host threads) race and must be ordered by the caller.
+ * Results equal frsdg_post_step's for the same configuration and input. */
+int frsdg_post_step_static(const frsdg_config* cfg, double* U, void* stream);
+
 /* Host-only set-up operators, usable without a GPU.
  * Reference element: GLL (reference_element.hpp:50-147) and CachedElementData
  * (cached_computations.hpp:225-334).  Arrays: nodes[n], weights[n], D[n*n]
