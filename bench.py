@@ -28,7 +28,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "DOF-residuals/s (FP64 FR residual, rhs_func)"
 UNIT = "DOF-residuals/s"
-WORKLOAD = "blast_vdw_1024x1024_p5 (2D radial blast, HLLC, Van der Waals a=0.05 b=0.02, filter + shock sensor)"
+WORKLOAD = "blast_vdw_1024x1024_p5 (2D radial blast, HLLC, Van der Waals a=0.05 b=0.02, WENO + shock sensor)"
 
 
 def dist_env():
@@ -261,6 +261,59 @@ def run_ours(args, ws, rank, local):
             "traffic": traffic_per_launch(), "peak_kind": peak_kind, "kernel": "fr2d_kernel<double,6,VdW,HLLC,affine>",
             "algorithmic_bytes_per_launch": alg_bytes, "mean_launch_ms": mean_launch_s * 1e3}
 
+    # ---- time to t_end.  (1) The blast's own schedule (SSP-RK3, 200 steps, WENO with
+    # the shock sensor), a throughput figure: the reference algorithm itself turns this
+    # configuration non-finite (no positivity limiter), so it is not a converged run.
+    # (2) The curved isentropic vortex (64^2, p = 4, RK4, CFL 0.05) to t = 10 with its
+    # L2 density error against the exact translated vortex.
+    t_end = None
+    if not args.no_t_end:
+        from fr_sdg_b200.integrate import Integrator, cfl_time_step, l2_error, node_jacobian
+        from fr_sdg_b200.workloads import exact_vortex, node_coords, pack2d, vortex_curved
+
+        def timed(fn):
+            barrier()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            res = fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+            ms = e0.elapsed_time(e1)
+            if dist:
+                tt = torch.tensor([ms], device=f"cuda:{local}")
+                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+                ms = float(tt.item())
+            return res, ms
+
+        U1 = wl.init(f"cuda:{local}")
+        dt = cfl_time_step(wl.cfg, U1, wl.cfl)
+        integ = Integrator(solver, "ssprk3")
+        integ.step(U1, 0.0, dt)  # warm (allocates the stage buffers)
+        U1.copy_(wl.init(f"cuda:{local}"))
+        solver.status()
+        st, ms = timed(lambda: integ.run(U1, dt, n_steps=wl.n_steps))
+        blast = {"seconds": ms / 1e3, "steps": st.steps, "dt": dt, "scheme": "SSP-RK3 + WENO/shock sensor",
+                 "stage_dof_residuals_per_s": ws * dofs * 3 * st.steps / (ms / 1e3),
+                 "finite": solver.status() == 0}
+        del U1, integ
+        vw = vortex_curved()
+        with FRSolver(vw.cfg) as vs:
+            V = vw.init(f"cuda:{local}")
+            vdt = cfl_time_step(vw.cfg, V, vw.cfl)
+            vint = Integrator(vs, "rk4")
+            vint.step(V, 0.0, vdt)
+            V.copy_(vw.init(f"cuda:{local}"))
+            vst, vms = timed(lambda: vint.run(V, vdt, t_end=vw.t_end))
+            x, y = node_coords(vw.cfg, f"cuda:{local}")
+            err = l2_error(vw.cfg, V, pack2d(*exact_vortex(vst.t, x, y)), node_jacobian(vw.cfg, V.device))
+            vortex = {"workload": vw.name, "seconds": vms / 1e3, "steps": vst.steps, "t_end": vst.t, "dt": vdt,
+                      "scheme": "RK4", "l2_density_error_vs_exact": float(err[0]),
+                      "finite": vs.status() == 0}
+        t_end = {"vortex_curved_64x64_p4": vortex, "blast_200_steps": blast}
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import oracle
@@ -288,7 +341,7 @@ def run_ours(args, ws, rank, local):
                    "l2": f"inputs ({dofs * 8 / 1e9:.2f} GB) larger than L2 (126 MB); no flush",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
         "clocks": clk.summary(), "gpu_launches": args.steps, "roofline": roof, "e2e": e2e,
-        "cpu_baseline": cpu, "bad_density_nodes": bad,
+        "cpu_baseline": cpu, "bad_density_nodes": bad, "time_to_t_end": t_end,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -304,6 +357,7 @@ def main(argv=None):
     ap.add_argument("--elements", type=int, default=1024, help="elements per direction (1024 = the workload)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-t-end", action="store_true", help="skip the 200-step time-to-t_end run")
     ap.add_argument("--cpu-all-cores", action="store_true")
     args = ap.parse_args(argv)
     if args.warmup < 3 and args.impl == "ours":

@@ -65,6 +65,7 @@ SIGNATURES = {
     "frsdg_ifunction": (C.c_int, [_P, _D, _P, _P, _P, _P]),
     "frsdg_jvp_prepare": (C.c_int, [_P, _D, _D, _P]),
     "frsdg_jvp": (C.c_int, [_P, _P, _P, _P]),
+    "frsdg_rk_stage": (C.c_int, [_P, _D, _P, _P, _D, _P, _D, _D, _P, _P, _D, _P]),
     "frsdg_post_step": (C.c_int, [_P, _P, _P]),
     "frsdg_post_step_static": (C.c_int, [C.POINTER(frsdg_config), _P, _P]),
     "frsdg_prim_to_cons": (C.c_int, [_P, _P, _P, _P]),

@@ -481,7 +481,8 @@ int frsdg_n_dofs(const frsdg_handle* h, int64_t* n)
 
 namespace
 {
-int run_residual(frsdg_handle* h, int mode, double t, const double* U, const double* W, double* out, void* stream)
+int run_residual(frsdg_handle* h, int mode, double t, const double* U, const double* W, double* out, void* stream,
+                 const StageArgs* stage = nullptr)
 {
     if (!h || !U || !out) return fail(FRSDG_ERR_ARG, "null argument");
     if ((reinterpret_cast<uintptr_t>(U) | reinterpret_cast<uintptr_t>(out)) & 15)
@@ -503,6 +504,7 @@ int run_residual(frsdg_handle* h, int mode, double t, const double* U, const dou
         a.h = hh;
         a.inv_h = 1.0 / hh;
         a.sigma = h->jvp_sigma;
+        if (stage) a.st = *stage;
         if (mode == MODE_JVP) e = dispatch2d<cplx>(h->n, h->cfg.gas_law, h->cfg.riemann, h->geo, a, s);
         else e = dispatch2d<double>(h->n, h->cfg.gas_law, h->cfg.riemann, h->geo, a, s);
     }
@@ -518,6 +520,7 @@ int run_residual(frsdg_handle* h, int mode, double t, const double* U, const dou
         a.h = hh;
         a.inv_h = 1.0 / hh;
         a.sigma = h->jvp_sigma;
+        if (stage) a.st = *stage;
         if (mode == MODE_JVP) e = dispatch1d<cplx>(h->n, h->cfg.gas_law, h->cfg.riemann, a, s);
         else e = dispatch1d<double>(h->n, h->cfg.gas_law, h->cfg.riemann, a, s);
     }
@@ -542,6 +545,15 @@ int frsdg_ifunction(frsdg_handle* h, double t, const double* U, const double* U_
 {
     if (!U_t) return fail(FRSDG_ERR_ARG, "null U_t");
     return run_residual(h, MODE_IFUNC, t, U, U_t, F, stream);
+}
+
+int frsdg_rk_stage(frsdg_handle* h, double t, const double* Us, const double* A, double alpha, const double* B,
+                   double beta, double gamma, double* out, double* acc, double delta, void* stream)
+{
+    if (!h || !Us || !out) return fail(FRSDG_ERR_ARG, "null argument");
+    if (out == Us) return fail(FRSDG_ERR_ARG, "frsdg_rk_stage: out must not alias Us");
+    StageArgs st{A, B, acc, alpha, beta, gamma, delta};
+    return run_residual(h, MODE_STAGE, t, Us, nullptr, out, stream, &st);
 }
 
 int frsdg_jvp_prepare(frsdg_handle* h, double t, double sigma, const double* U)

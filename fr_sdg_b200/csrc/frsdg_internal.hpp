@@ -17,7 +17,17 @@ enum Mode : int
     MODE_RESIDUAL = 0, // R(U)                      residual_kernel<double>
     MODE_RHS      = 1, // -R(U)                     rhs_func
     MODE_IFUNC    = 2, // U_t + R(M(U))             fun_implicit
-    MODE_JVP      = 3  // sigma Im(u)/h + Im(R)/h   ComplexStepJacobianStrategy::matmult
+    MODE_JVP      = 3, // sigma Im(u)/h + Im(R)/h   ComplexStepJacobianStrategy::matmult
+    MODE_STAGE    = 4  // out = alpha A + beta B + gamma rhs, acc += delta rhs (rhs = -R): one RK stage
+};
+
+// Explicit Runge-Kutta stage fused into the residual's output pass.
+struct StageArgs
+{
+    const double* A;   // may be null (term dropped)
+    const double* B;   // may be null
+    double*       acc; // may be null
+    double alpha, beta, gamma, delta;
 };
 
 // Geometry classes of the 2D kernel: constant diagonal metrics (Cartesian and the
@@ -68,6 +78,7 @@ struct Fr2dArgs
     void*  out;        // double* (float* for the FP32 residual)
     double h, inv_h, sigma;
     unsigned long long* bad;
+    StageArgs st;
     Ops    ops;
 };
 
@@ -85,6 +96,7 @@ struct Fr1dArgs
     void*  out;
     double h, inv_h, sigma;
     unsigned long long* bad;
+    StageArgs st;
     Ops    ops;
 };
 
@@ -111,5 +123,23 @@ __host__ __device__ constexpr int tile_y(int n)
 // Launchers (one translation unit per polynomial order).
 template <class S, int N> cudaError_t launch_fr2d(int gas, int riem, int geo, const Fr2dArgs& a, cudaStream_t s);
 template <class S, int N> cudaError_t launch_fr1d(int gas, int riem, const Fr1dArgs& a, cudaStream_t s);
+
+// Output of one real residual value r = R at index idx in the requested form.
+__device__ __forceinline__ void store_residual(int mode, const double* W, const StageArgs& st, double* out,
+                                               int64_t idx, double r)
+{
+    if (mode == MODE_RHS) out[idx] = -r;
+    else if (mode == MODE_IFUNC) out[idx] = __ldg(W + idx) + r;
+    else if (mode == MODE_STAGE)
+    {
+        const double v = -r;
+        double o = 0.0;
+        if (st.A) o = st.alpha * __ldg(st.A + idx);
+        if (st.B) o = o + st.beta * __ldg(st.B + idx);
+        out[idx] = o + st.gamma * v;
+        if (st.acc) st.acc[idx] = st.acc[idx] + st.delta * v;
+    }
+    else out[idx] = r;
+}
 
 } // namespace frsdg

@@ -150,11 +150,7 @@ __global__ void __launch_bounds__(kThreads) fr1d_kernel(const Fr1dArgs a)
         }
         else
         {
-            double v;
-            if (a.mode == MODE_RHS) v = -s_re(r);
-            else if (a.mode == MODE_IFUNC) v = __ldg(a.W + gidx) + s_re(r);
-            else v = s_re(r);
-            reinterpret_cast<double*>(a.out)[gidx] = v;
+            store_residual(a.mode, a.W, a.st, reinterpret_cast<double*>(a.out), gidx, s_re(r));
         }
     }
 }

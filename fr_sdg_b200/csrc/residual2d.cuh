@@ -550,10 +550,7 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
             }
             else
             {
-                const double r = s_re(R);
-                if (a.mode == MODE_RHS) out[gidx] = -r;
-                else if (a.mode == MODE_IFUNC) out[gidx] = __ldg(a.W + gidx) + r;
-                else out[gidx] = r;
+                store_residual(a.mode, a.W, a.st, out, gidx, s_re(R));
             }
         }
     }

@@ -1,0 +1,154 @@
+"""Explicit time integration over the fused RK stages of libfrsdg.
+
+The reference hands time stepping to PETSc TS (petsc_solver_impl.hpp:549-612):
+SSP Runge-Kutta or classic RK4, the last step clipped to land on the final time
+(TS_EXACTFINALTIME_MATCHSTEP, 556), and the post-step stabilisation after every
+accepted step (604-607).  Here each stage is one frsdg_rk_stage call (residual
+and update in one pass over the state):
+
+  SSP-RK3 (Shu and Osher, J. Comput. Phys. 77, 1988):
+    U1 = U + dt L(U);  U2 = 3/4 U + 1/4 U1 + dt/4 L(U1);  U+ = 1/3 U + 2/3 U2 + 2 dt/3 L(U2)
+  RK4 (classic):  acc accumulates dt/6 (k1 + 2 k2 + 2 k3 + k4) on top of U.
+
+Time step: dt = CFL * (L/N) / c_max(U0), c_max the largest |velocity| + sound speed
+of the initial state (tools/run_test_matrix.py:40-52 take c_max as an input).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import torch
+
+from . import _abi as A
+from .solver import FRSolver
+
+
+def max_wave_speed(cfg: A.frsdg_config, U: torch.Tensor) -> float:
+    """max(|v| + c) over the nodes, c from the configured gas law."""
+    n = cfg.poly_deg + 1
+    if cfg.dim == 2:
+        q = U.view(-1, 4)
+        rho, ru, rv, E = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    else:
+        q = U.view(-1, 3, n)
+        rho, ru, E = q[:, 0], q[:, 1], q[:, 2]
+        rv = torch.zeros_like(rho)
+    u, v = ru / rho, rv / rho
+    e = E / rho - 0.5 * (u * u + v * v)
+    g = cfg.gamma
+    if cfg.gas_law == A.GAS_IDEAL:
+        c2 = g * (g - 1.0) * e
+    else:
+        a, b = cfg.vdw_a, cfg.vdw_b
+        cov = 1.0 - b * rho
+        c2 = (g * (g - 1.0) * (e + a * rho)) / (cov * cov) + ((g - 1.0) * a * rho * (2.0 - b * rho)) / (cov * cov) \
+            - 2.0 * a * rho
+    return float((torch.sqrt(u * u + v * v) + torch.sqrt(c2)).max())
+
+
+def cfl_time_step(cfg: A.frsdg_config, U0: torch.Tensor, cfl: float) -> float:
+    h = cfg.box_length[0] / cfg.n_elems[0]
+    if cfg.dim == 2:
+        h = min(h, cfg.box_length[1] / cfg.n_elems[1])
+    return cfl * h / max_wave_speed(cfg, U0)
+
+
+@dataclass
+class RunStats:
+    steps: int
+    t: float
+    dt: float
+
+
+class Integrator:
+    """SSP-RK3 / RK4 over one FRSolver; buffers are allocated once."""
+
+    def __init__(self, solver: FRSolver, scheme: str = "ssprk3"):
+        if scheme not in ("ssprk3", "rk4"):
+            raise ValueError("scheme must be 'ssprk3' or 'rk4'")
+        self.s = solver
+        self.scheme = scheme
+        self._buf = None
+        cfg = solver.cfg
+        self.stabilise = bool(cfg.apply_filter or cfg.apply_weno)
+
+    def _buffers(self, U: torch.Tensor):
+        if self._buf is None or self._buf[0].device != U.device:
+            self._buf = [torch.empty_like(U) for _ in range(3)]
+        return self._buf
+
+    def step(self, U: torch.Tensor, t: float, dt: float) -> None:
+        """Advance U (in place) from t to t + dt, then apply the post-step limiter."""
+        s = self.s
+        b1, b2, b3 = self._buffers(U)
+        if self.scheme == "ssprk3":
+            s.rk_stage(t, U, b1, gamma=dt, a=U, alpha=1.0)
+            s.rk_stage(t + dt, b1, b2, gamma=0.25 * dt, a=U, alpha=0.75, b=b1, beta=0.25)
+            s.rk_stage(t + 0.5 * dt, b2, U, gamma=2.0 * dt / 3.0, a=U, alpha=1.0 / 3.0, b=b2, beta=2.0 / 3.0)
+        else:
+            b3.copy_(U)
+            s.rk_stage(t, U, b1, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 6.0)
+            s.rk_stage(t + 0.5 * dt, b1, b2, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
+            s.rk_stage(t + 0.5 * dt, b2, b1, gamma=dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
+            s.rk_stage(t + dt, b1, U, gamma=dt / 6.0, a=b3, alpha=1.0)
+        if self.stabilise:
+            s.apply_stabilization(U)
+
+    def run(self, U: torch.Tensor, dt: float, t_end: float | None = None, n_steps: int | None = None,
+            t0: float = 0.0) -> RunStats:
+        """March to t_end (last step clipped to land on it) or for n_steps steps."""
+        t, k = t0, 0
+        if t_end is not None:
+            while t < t_end - 1e-14 * max(1.0, abs(t_end)):
+                h = min(dt, t_end - t)
+                self.step(U, t, h)
+                t += h
+                k += 1
+        else:
+            for _ in range(int(n_steps)):
+                self.step(U, t, dt)
+                t += dt
+                k += 1
+        return RunStats(k, t, dt)
+
+
+def node_jacobian(cfg: A.frsdg_config, device="cpu") -> torch.Tensor:
+    """detJ of the map (r, s) -> (x, y) at every node, [elem][l][k] flattened, for the
+    Cartesian and sine-warped geometries (physics_evaluator.hpp:282-305)."""
+    from .refelem import reference_element
+
+    Nx, Ny, n = cfg.n_elems[0], cfg.n_elems[1], cfg.poly_deg + 1
+    Lx, Ly = cfg.box_length[0], cfg.box_length[1]
+    xr = torch.tensor(reference_element(cfg.poly_deg)[0], dtype=torch.float64, device=device)
+    i = torch.arange(Nx, dtype=torch.float64, device=device)
+    j = torch.arange(Ny, dtype=torch.float64, device=device)
+    csi = (i[None, :, None, None] + 0.5 * (1 + xr[None, None, None, :])) / Nx
+    eta = (j[:, None, None, None] + 0.5 * (1 + xr[None, None, :, None])) / Ny
+    if cfg.geometry == A.GEOM_SINE_WARP:
+        two_pi, amp = 2.0 * math.pi, cfg.geom_params[0]
+        dc = two_pi * amp * torch.cos(two_pi * csi) * torch.sin(two_pi * eta)
+        de = two_pi * amp * torch.sin(two_pi * csi) * torch.cos(two_pi * eta)
+        det = (Lx + dc) * (Ly + de) - de * dc
+    elif cfg.geometry == A.GEOM_CARTESIAN:
+        det = torch.full_like(csi * eta, Lx * Ly)
+    else:
+        raise NotImplementedError("node_jacobian: Cartesian and sine-warp geometries only")
+    det = det * (0.5 / Nx) * (0.5 / Ny)
+    return det.expand(Ny, Nx, n, n).reshape(-1)
+
+
+def l2_error(cfg: A.frsdg_config, U: torch.Tensor, exact: torch.Tensor, detJ: torch.Tensor | float = 1.0) -> torch.Tensor:
+    """GLL-quadrature L2 error per conserved variable (compute_error,
+    physics_impl_2D.hpp:203-265 / physics_impl_1D.hpp:245-324)."""
+    from .refelem import reference_element
+
+    n = cfg.poly_deg + 1
+    w = torch.tensor(reference_element(cfg.poly_deg)[1], dtype=torch.float64, device=U.device)
+    if cfg.dim == 2:
+        d = (U - exact).view(-1, n, n, 4)
+        wt = (w[:, None] * w[None, :])[None, :, :, None] * (detJ if isinstance(detJ, float) else detJ.view(-1, n, n, 1))
+        return torch.sqrt((wt * d * d).sum(dim=(0, 1, 2)))
+    d = (U - exact).view(-1, 3, n)
+    jac = 0.5 * cfg.box_length[0] / cfg.n_elems[0]
+    return torch.sqrt((w[None, None, :] * jac * d * d).sum(dim=(0, 2)))

@@ -72,6 +72,15 @@ class FRSolver:
         self._check_vec(U, U_t, F)
         A.check(self._lib.frsdg_ifunction(self._h, t, _ptr(U), _ptr(U_t), _ptr(F), _stream()), "frsdg_ifunction")
 
+    def rk_stage(self, t: float, Us: torch.Tensor, out: torch.Tensor, gamma: float,
+                 a: torch.Tensor | None = None, alpha: float = 0.0, b: torch.Tensor | None = None,
+                 beta: float = 0.0, acc: torch.Tensor | None = None, delta: float = 0.0) -> None:
+        """out = alpha a + beta b + gamma rhs(Us); acc += delta rhs(Us) -- one fused RK stage."""
+        self._check_vec(Us, out, *(v for v in (a, b, acc) if v is not None))
+        p = lambda v: _ptr(v) if v is not None else None
+        A.check(self._lib.frsdg_rk_stage(self._h, t, _ptr(Us), p(a), alpha, p(b), beta, gamma, _ptr(out),
+                                         p(acc), delta, _stream()), "frsdg_rk_stage")
+
     def pre_jv_eval(self, t: float, U: torch.Tensor, sigma: float) -> None:
         self._check_vec(U)
         self._jvp_U = U  # keep alive while the library holds the pointer

@@ -159,10 +159,21 @@ class Workload:
         return self.n_nodes * (self.cfg.dim + 2)
 
 
+# Stabilisation of the shock runs.  The reference's factory puts the interface node at
+# x = 0.5 on the right state (factory.hpp:199), so the jump starts inside an element;
+# with the spectral filter alone the reference algorithm (and the oracle restating it)
+# produces NaN within the first steps at any CFL, and with filter and WENO both on the
+# WENO result is overwritten by the filter (filter.hpp:733-742).  Full runs therefore use
+# the reference tools' own shock settings: WENO with the shock sensor, filter off
+# (tools/check_radial.py:221-236), at a CFL below the explicit ceilings those tools
+# measured (tools/cfl_ceiling_shock.py:32-35).
+SHOCK_STAB = dict(apply_filter=False, apply_weno=True, weno_gamma=0.998, threshold=0.8, theta=1.0)
+
+
 def sod1d(n_elems: int = 200, p: int = 3) -> Workload:
-    """1D Sod tube: [0,1], Rusanov, DG (c=0), filter, SSP-RK3, CFL 0.1, t_end 0.2."""
+    """1D Sod tube: [0,1], Rusanov, DG (c=0), SSP-RK3 to t_end 0.2, WENO + shock sensor."""
     cfg = make_config(dim=1, p=p, n_elems=(n_elems, 1), box=(1.0, 1.0), riemann="rusanov",
-                      bcs={A.LEFT: A.BC_OUTFLOW, A.RIGHT: A.BC_OUTFLOW}, apply_filter=True)
+                      bcs={A.LEFT: A.BC_OUTFLOW, A.RIGHT: A.BC_OUTFLOW}, **SHOCK_STAB)
 
     def init(device="cpu"):
         x, _ = node_coords(cfg, device)
@@ -172,7 +183,7 @@ def sod1d(n_elems: int = 200, p: int = 3) -> Workload:
         zero = torch.zeros_like(rho)
         return pack1d(rho, zero, rhoE("ideal", 1.4, 0, 0, rho, zero, p_))
 
-    return Workload("sod1d_n200_p3", cfg, "ssprk3", 0.1, 0.2, None, init)
+    return Workload(f"sod1d_n{n_elems}_p{p}", cfg, "ssprk3", 0.025, 0.2, None, init)
 
 
 def vortex_curved(n_elems: int = 64, p: int = 4, amplitude: float = 0.1) -> Workload:
@@ -186,7 +197,8 @@ def vortex_curved(n_elems: int = 64, p: int = 4, amplitude: float = 0.1) -> Work
         x, y = node_coords(cfg, device)
         return pack2d(*exact_vortex(0.0, x, y))
 
-    return Workload(f"vortex_sinewarp_{n_elems}x{n_elems}_p{p}", cfg, "rk4", None, 10.0, None, init)
+    # CFL 0.05: RK4 with p = 4 on the warped mesh diverges at 0.1 (checked with the oracle)
+    return Workload(f"vortex_sinewarp_{n_elems}x{n_elems}_p{p}", cfg, "rk4", 0.05, 10.0, None, init)
 
 
 def bump_channel(nx: int = 256, ny: int = 64, p: int = 3, mach: float = 0.5) -> Workload:
@@ -221,13 +233,13 @@ def bump_channel(nx: int = 256, ny: int = 64, p: int = 3, mach: float = 0.5) -> 
 
 def blast_large(n_elems: int = 1024, p: int = 5) -> Workload:
     """2D radial blast on [0,1]^2, HLLC, Van der Waals (a=0.05, b=0.02, gamma=1.4),
-    filter with shock sensor, SSP-RK3, CFL 0.1, 200 steps."""
+    SSP-RK3, 200 steps, WENO + shock sensor (CFL 0.01: p = 5)."""
     a, b, g = 0.05, 0.02, 1.4
     cfg = make_config(dim=2, p=p, n_elems=(n_elems, n_elems), box=(1.0, 1.0), riemann="hllc",
                       gas="vdw", gamma=g, vdw=(a, b),
                       bcs={A.LEFT: A.BC_OUTFLOW, A.RIGHT: A.BC_OUTFLOW, A.TOP: A.BC_OUTFLOW,
                            A.BOTTOM: A.BC_OUTFLOW},
-                      apply_filter=True, apply_weno=True)
+                      **SHOCK_STAB)
 
     def init(device="cpu"):
         x, y = node_coords(cfg, device)
@@ -238,7 +250,7 @@ def blast_large(n_elems: int = 1024, p: int = 5) -> Workload:
         zero = torch.zeros_like(rho)
         return pack2d(rho, zero, zero, rhoE("vdw", g, a, b, rho, zero, pr))
 
-    return Workload(f"blast_vdw_{n_elems}x{n_elems}_p{p}", cfg, "ssprk3", 0.1, None, 200, init)
+    return Workload(f"blast_vdw_{n_elems}x{n_elems}_p{p}", cfg, "ssprk3", 0.01, None, 200, init)
 
 
 def circular_explosion(n_elems: int, p: int, gas: str, gamma: float, vdw, r0: float, p_out: float,

@@ -169,6 +169,16 @@ int frsdg_jvp_prepare(frsdg_handle* h, double t, double sigma, const double* U);
  * ComplexStepJacobianStrategy::matmult (petsc_solver_impl.hpp:250-432). */
 int frsdg_jvp(frsdg_handle* h, const double* V, double* JV, void* stream);
 
+/* One explicit Runge-Kutta stage fused into the residual pass:
+ *   out = alpha*A + beta*B + gamma*rhs(Us),   acc += delta*rhs(Us)   (rhs = -R)
+ * A, B and acc may be NULL (the term is dropped).  out must not alias Us (the
+ * residual reads neighbouring elements of Us while out is written); A, B and acc may
+ * alias each other or out.  SSP-RK3 and classic RK4 are sequences of such stages;
+ * the reference delegates them to PETSc TS (petsc_solver_impl.hpp:549-612). */
+int frsdg_rk_stage(frsdg_handle* h, double t, const double* Us, const double* A, double alpha,
+                   const double* B, double beta, double gamma, double* out, double* acc, double delta,
+                   void* stream);
+
 /* In-place post-step stabilisation U <- limit(U) (spectral filter, WENO with
  * shock sensor): PetscSolver::apply_stabilization (petsc_solver_impl.hpp:683-702). */
 int frsdg_post_step(frsdg_handle* h, double* U, void* stream);
