@@ -45,7 +45,7 @@ class frsdg_config(C.Structure):
         ("apply_weno", C.c_int32),
         ("filt_alpha", C.c_double), ("weno_gamma", C.c_double),
         ("shock_theta", C.c_double), ("shock_threshold", C.c_double),
-        ("cond_sys", C.c_int32), ("pad1_", C.c_int32),
+        ("cond_sys", C.c_int32), ("jvp_exact_bc", C.c_int32),
         ("csd_eps", C.c_double),
     ]
 
@@ -66,6 +66,9 @@ SIGNATURES = {
     "frsdg_jvp_prepare": (C.c_int, [_P, _D, _D, _P]),
     "frsdg_jvp": (C.c_int, [_P, _P, _P, _P]),
     "frsdg_rk_stage": (C.c_int, [_P, _D, _P, _P, _D, _P, _D, _D, _P, _P, _D, _P]),
+    "frsdg_jac_blocks": (C.c_int, [_P, _D, _D, _P, _P, _P]),
+    "frsdg_pc_setup": (C.c_int, [_P, _D, _D, _P, _P]),
+    "frsdg_pc_apply": (C.c_int, [_P, _P, _P, _P]),
     "frsdg_post_step": (C.c_int, [_P, _P, _P]),
     "frsdg_post_step_static": (C.c_int, [C.POINTER(frsdg_config), _P, _P]),
     "frsdg_prim_to_cons": (C.c_int, [_P, _P, _P, _P]),

@@ -8,6 +8,7 @@
 #include "device_math.cuh"
 #include "frsdg_internal.hpp"
 #include "setup_ops.hpp"
+#include "jacobi.hpp"
 #include "stab.hpp"
 
 #include <cmath>
@@ -142,6 +143,9 @@ struct frsdg_handle
     double*      d_work = nullptr;   // post-step source copy (WENO)
     double*      d_stage = nullptr;  // host-buffer staging (2 * ntot), allocated on first use
     unsigned long long* d_bad = nullptr;
+    double*      d_blocks = nullptr;  // preconditioner: element-diagonal Jacobian blocks (FP64)
+    float*       d_inv = nullptr;     // and their inverses (FP32); both allocated by the first frsdg_pc_setup
+    unsigned long long* d_singular = nullptr;
     double       jvp_t = 0.0, jvp_sigma = 1.0;
     const double* jvp_U = nullptr;
     cudaStream_t last = nullptr;
@@ -158,6 +162,9 @@ static void free_handle(frsdg_handle* h)
     cudaFree(h->d_work);
     cudaFree(h->d_stage);
     cudaFree(h->d_bad);
+    cudaFree(h->d_blocks);
+    cudaFree(h->d_inv);
+    cudaFree(h->d_singular);
     delete h;
 }
 
@@ -318,6 +325,9 @@ int frsdg_create(const frsdg_config* cfg, frsdg_handle** out)
         a.Ly = cfg->box_length[1];
         a.ops = ops;
         a.bad = h->d_bad;
+        a.nd = 4 * n * n;
+        a.exact_bc = cfg->jvp_exact_bc;
+        a.jac_cmode = ((per_x && (Nx & 1)) || (per_y && (Ny & 1))) ? 1 : 0;
         for (int d = 0; d < 4; ++d)
         {
             a.bc[d].kind = cfg->bc[d].kind;
@@ -544,6 +554,7 @@ int frsdg_rhs(frsdg_handle* h, double t, const double* U, double* rhs, void* str
 int frsdg_ifunction(frsdg_handle* h, double t, const double* U, const double* U_t, double* F, void* stream)
 {
     if (!U_t) return fail(FRSDG_ERR_ARG, "null U_t");
+    if (reinterpret_cast<uintptr_t>(U_t) & 15) return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
     return run_residual(h, MODE_IFUNC, t, U, U_t, F, stream);
 }
 
@@ -552,6 +563,8 @@ int frsdg_rk_stage(frsdg_handle* h, double t, const double* Us, const double* A,
 {
     if (!h || !Us || !out) return fail(FRSDG_ERR_ARG, "null argument");
     if (out == Us) return fail(FRSDG_ERR_ARG, "frsdg_rk_stage: out must not alias Us");
+    if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(acc)) & 15)
+        return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
     StageArgs st{A, B, acc, alpha, beta, gamma, delta};
     return run_residual(h, MODE_STAGE, t, Us, nullptr, out, stream, &st);
 }
@@ -571,6 +584,71 @@ int frsdg_jvp(frsdg_handle* h, const double* V, double* JV, void* stream)
     if (!h->jvp_U) return fail(FRSDG_ERR_ARG, "frsdg_jvp called before frsdg_jvp_prepare");
     if (reinterpret_cast<uintptr_t>(V) & 15) return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
     return run_residual(h, MODE_JVP, h->jvp_t, h->jvp_U, V, JV, stream);
+}
+
+int frsdg_jac_blocks(frsdg_handle* h, double t, double sigma, const double* U, double* blocks, void* stream)
+{
+    if (!h || !U || !blocks) return fail(FRSDG_ERR_ARG, "null argument");
+    if (h->cfg.dim != 2) return fail(FRSDG_ERR_UNSUPPORTED, "frsdg_jac_blocks: 2D configurations only");
+    if ((reinterpret_cast<uintptr_t>(U) | reinterpret_cast<uintptr_t>(blocks)) & 15)
+        return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    h->last = s;
+    Fr2dArgs a = h->a2;
+    a.t = t;
+    a.mode = MODE_JAC;
+    a.cond_sys = h->cfg.cond_sys;
+    a.U = U;
+    a.W = nullptr;
+    a.out = blocks;
+    a.h = h->cfg.csd_eps;
+    a.inv_h = 1.0 / h->cfg.csd_eps;
+    a.sigma = sigma;
+    const cudaError_t e = dispatch2d<cplx>(h->n, h->cfg.gas_law, h->cfg.riemann, h->geo, a, s);
+    if (e != cudaSuccess) return cuda_fail(e, "Jacobian-block launch");
+    return FRSDG_OK;
+}
+
+int frsdg_pc_setup(frsdg_handle* h, double t, double sigma, const double* U, void* stream)
+{
+    if (!h || !U) return fail(FRSDG_ERR_ARG, "null argument");
+    if (h->cfg.dim != 2) return fail(FRSDG_ERR_UNSUPPORTED, "frsdg_pc_setup: 2D configurations only");
+    const int nd = h->ndofs;
+    if (nd > kMaxBlockDofs) return fail(FRSDG_ERR_UNSUPPORTED, "frsdg_pc_setup: element blocks above 144 DOFs (p > 5)");
+    cudaError_t e;
+    if (!h->d_blocks)
+    {
+        const size_t nb = size_t(h->nelem) * nd * nd;
+        if ((e = cudaMalloc(&h->d_blocks, sizeof(double) * nb)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(blocks)");
+        if ((e = cudaMalloc(&h->d_inv, sizeof(float) * nb)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(inverse blocks)");
+        if ((e = cudaMalloc(&h->d_singular, sizeof(unsigned long long))) != cudaSuccess)
+            return cuda_fail(e, "cudaMalloc(pivot flag)");
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if ((e = cudaMemsetAsync(h->d_singular, 0, sizeof(unsigned long long), s)) != cudaSuccess)
+        return cuda_fail(e, "cudaMemsetAsync");
+    int rc = frsdg_jac_blocks(h, t, sigma, U, h->d_blocks, stream);
+    if (rc) return rc;
+    if ((e = launch_block_inverse(h->d_blocks, h->d_inv, nd, h->nelem, h->d_singular, s)) != cudaSuccess)
+        return cuda_fail(e, "block-inverse launch");
+    unsigned long long nsing = 0;
+    if ((e = cudaMemcpyAsync(&nsing, h->d_singular, sizeof(nsing), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return cuda_fail(e, "pivot flag read");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "pc setup sync");
+    if (nsing) return fail(FRSDG_ERR_ARG, "frsdg_pc_setup: singular element block (zero pivot)");
+    return FRSDG_OK;
+}
+
+int frsdg_pc_apply(frsdg_handle* h, const double* r, double* z, void* stream)
+{
+    if (!h || !r || !z) return fail(FRSDG_ERR_ARG, "null argument");
+    if (!h->d_inv) return fail(FRSDG_ERR_ARG, "frsdg_pc_apply called before frsdg_pc_setup");
+    if (r == z) return fail(FRSDG_ERR_ARG, "frsdg_pc_apply: z must not alias r");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    h->last = s;
+    const cudaError_t e = launch_block_apply(h->d_inv, r, z, h->ndofs, h->nelem, s);
+    if (e != cudaSuccess) return cuda_fail(e, "block-apply launch");
+    return FRSDG_OK;
 }
 
 int frsdg_post_step(frsdg_handle* h, double* U, void* stream)

@@ -76,6 +76,8 @@ __device__ __forceinline__ cplx s_sqrt(cplx z)
     if (z.re >= 0.0) return {t, z.im / (2.0 * t)};
     return {fabs(z.im) / (2.0 * t), copysign(t, z.im)};
 }
+__device__ __forceinline__ double s_log(double x) { return log(x); }
+__device__ __forceinline__ cplx s_log(cplx z) { return {log(hypot(z.re, z.im)), atan2(z.im, z.re)}; }
 __device__ __forceinline__ double s_exp(double x) { return exp(x); }
 __device__ __forceinline__ float s_exp(float x) { return expf(x); }
 __device__ __forceinline__ cplx s_exp(cplx z)

@@ -18,7 +18,8 @@ enum Mode : int
     MODE_RHS      = 1, // -R(U)                     rhs_func
     MODE_IFUNC    = 2, // U_t + R(M(U))             fun_implicit
     MODE_JVP      = 3, // sigma Im(u)/h + Im(R)/h   ComplexStepJacobianStrategy::matmult
-    MODE_STAGE    = 4  // out = alpha A + beta B + gamma rhs, acc += delta rhs (rhs = -R): one RK stage
+    MODE_STAGE    = 4, // out = alpha A + beta B + gamma rhs, acc += delta rhs (rhs = -R): one RK stage
+    MODE_JAC      = 5  // element-diagonal blocks of sigma dM/dU + dR(M(U))/dU, coloured complex step
 };
 
 // Explicit Runge-Kutta stage fused into the residual's output pass.
@@ -79,8 +80,22 @@ struct Fr2dArgs
     double h, inv_h, sigma;
     unsigned long long* bad;
     StageArgs st;
+    int    nd;         // DOFs per element, 4 n^2
+    int    exact_bc;   // complex scalars: differentiate the user-lambda boundary kinds too
+    int    jac_cmode;  // MODE_JAC colouring: 0 checkerboard, 1 three-colour cycles (odd periodic)
     Ops    ops;
 };
+
+// Colour of element (gi, gj) for the coloured Jacobian: no two elements sharing a
+// face have the same colour.  Checkerboard, or, when a periodic direction has an
+// odd number of elements, (i mod 2 | 2 for the last) + 3 (j mod 2 | 2 for the last).
+__host__ __device__ inline int elem_colour(int cmode, int Nx, int Ny, int per_x, int per_y, int gi, int gj)
+{
+    if (cmode == 0) return (gi + gj) & 1;
+    const int cx = (per_x && (Nx & 1) && gi == Nx - 1) ? 2 : (gi & 1);
+    const int cy = (per_y && (Ny & 1) && gj == Ny - 1) ? 2 : (gj & 1);
+    return cx + 3 * cy;
+}
 
 struct Fr1dArgs
 {

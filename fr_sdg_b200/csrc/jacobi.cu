@@ -1,0 +1,154 @@
+// jacobi.cu -- element block-Jacobi preconditioner of the implicit path.
+//
+// The reference preconditions its matrix-free Newton-Krylov solve with a
+// finite-difference Jacobian assembled by DMDA colouring (MatFDColoringApply,
+// include/petsc_solver_impl.hpp:72-95 and 223-248).  Here the preconditioner is
+// the element-diagonal part of the same Jacobian, J_ee = sigma dM/dU + dR/dU,
+// from the coloured complex-step launch of the residual kernel (MODE_JAC), each
+// block inverted once per Newton step in FP64 and kept in FP32:
+//   block_inverse_kernel  Gauss-Jordan elimination with partial pivoting of one
+//                         column-major ND x ND block per CTA, in shared memory;
+//   block_apply_kernel    z_e = inv(J_ee) r_e, one CTA per element, FP64 sums.
+#include "jacobi.hpp"
+
+namespace frsdg
+{
+
+namespace
+{
+
+constexpr int kInvThreads = 256;
+
+// In-place inverse of the column-major n x n block A (a_ij at A[j n + i]) by
+// Gauss-Jordan elimination with row pivoting; the row exchanges are undone as
+// column exchanges at the end.  A zero pivot counts one singular block.
+__global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(const double* __restrict__ blocks, float* __restrict__ inv,
+                                                                    int n, unsigned long long* singular)
+{
+    extern __shared__ double sA[];  // n * n doubles, n doubles of column k, n ints of pivot rows
+    double* fcol = sA + n * n;
+    int* perm = reinterpret_cast<int*>(sA + n * n + n);
+    __shared__ int s_piv;
+    __shared__ double s_red_v[kInvThreads / 32];
+    __shared__ int s_red_i[kInvThreads / 32];
+    const int64_t base = int64_t(blockIdx.x) * n * n;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int q = tid; q < n * n; q += kInvThreads) sA[q] = blocks[base + q];
+    __syncthreads();
+    bool bad = false;
+    for (int k = 0; k < n; ++k)
+    {
+        // pivot: largest |a_ik|, i >= k (lowest index among equals)
+        double best = -1.0;
+        int bi = k;
+        for (int i = k + tid; i < n; i += kInvThreads)
+        {
+            const double v = fabs(sA[k * n + i]);
+            if (v > best) { best = v; bi = i; }
+        }
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            const double ov = __shfl_down_sync(0xffffffffu, best, o);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+        }
+        if (lane == 0) { s_red_v[warp] = best; s_red_i[warp] = bi; }
+        __syncthreads();
+        if (tid == 0)
+        {
+            double b = s_red_v[0];
+            int i0 = s_red_i[0];
+            for (int w = 1; w < kInvThreads / 32; ++w)
+                if (s_red_v[w] > b || (s_red_v[w] == b && s_red_i[w] < i0)) { b = s_red_v[w]; i0 = s_red_i[w]; }
+            s_piv = b > 0.0 ? i0 : -1;
+            perm[k] = b > 0.0 ? i0 : k;
+        }
+        __syncthreads();
+        const int pr = s_piv;
+        if (pr < 0)
+        {
+            bad = true;  // leave the block as it is; the caller reports the failure
+            break;
+        }
+        // exchange rows k and pr
+        if (pr != k)
+            for (int j = tid; j < n; j += kInvThreads)
+            {
+                const double t = sA[j * n + k];
+                sA[j * n + k] = sA[j * n + pr];
+                sA[j * n + pr] = t;
+            }
+        __syncthreads();
+        const double rp = 1.0 / sA[k * n + k];
+        // scale row k (its pivot entry becomes 1/a_kk); keep column k's multipliers
+        for (int j = tid; j < n; j += kInvThreads) sA[j * n + k] = (j == k ? 1.0 : sA[j * n + k]) * rp;
+        for (int i = tid; i < n; i += kInvThreads) fcol[i] = sA[k * n + i];
+        __syncthreads();
+        // eliminate column k from every other row: a_ij -= a_ik a_kj (a_ik -> -a_ik / a_kk)
+        for (int q = tid; q < n * n; q += kInvThreads)
+        {
+            const int j = q / n, i = q - j * n;
+            if (i == k) continue;
+            sA[q] = (j == k ? 0.0 : sA[q]) - fcol[i] * sA[j * n + k];
+        }
+        __syncthreads();
+    }
+    if (bad)
+    {
+        if (tid == 0 && singular) atomicAdd(singular, 1ull);
+        return;
+    }
+    // undo the row exchanges as column exchanges, last first
+    for (int k = n - 1; k >= 0; --k)
+    {
+        const int pr = perm[k];
+        if (pr != k)
+            for (int i = tid; i < n; i += kInvThreads)
+            {
+                const double t = sA[k * n + i];
+                sA[k * n + i] = sA[pr * n + i];
+                sA[pr * n + i] = t;
+            }
+        __syncthreads();
+    }
+    for (int q = tid; q < n * n; q += kInvThreads) inv[base + q] = static_cast<float>(sA[q]);
+}
+
+// z_e = inv_e r_e for every element e: one CTA per element, thread i owns row i.
+__global__ void block_apply_kernel(const float* __restrict__ inv, const double* __restrict__ r, double* __restrict__ z, int n)
+{
+    extern __shared__ double sr[];
+    const int64_t e = blockIdx.x;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) sr[j] = r[e * n + j];
+    __syncthreads();
+    const float* B = inv + e * int64_t(n) * n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+    {
+        double acc = 0.0;
+        for (int j = 0; j < n; ++j) acc = fma(static_cast<double>(__ldg(B + int64_t(j) * n + i)), sr[j], acc);
+        z[e * n + i] = acc;
+    }
+}
+
+} // namespace
+
+size_t block_inverse_smem(int n) { return size_t(n) * (n + 1) * sizeof(double) + size_t(n) * sizeof(int); }
+
+cudaError_t launch_block_inverse(const double* blocks, float* inv, int n, int64_t n_blocks, unsigned long long* singular,
+                                 cudaStream_t s)
+{
+    const size_t smem = block_inverse_smem(n);
+    cudaError_t e = cudaFuncSetAttribute(block_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    block_inverse_kernel<<<unsigned(n_blocks), kInvThreads, smem, s>>>(blocks, inv, n, singular);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_block_apply(const float* inv, const double* r, double* z, int n, int64_t n_blocks, cudaStream_t s)
+{
+    const int threads = n <= 64 ? 64 : n <= 128 ? 128 : 160;
+    block_apply_kernel<<<unsigned(n_blocks), threads, size_t(n) * sizeof(double), s>>>(inv, r, z, n);
+    return cudaGetLastError();
+}
+
+} // namespace frsdg

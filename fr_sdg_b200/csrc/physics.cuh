@@ -363,13 +363,83 @@ __device__ __forceinline__ void exact_vortex_dev(double time, double x, double y
     out[3] = (p / (gamma - 1.0)) + 0.5 * rho * (u * u + v * v);
 }
 
+// Complex-step ghost of the user-lambda kinds that depend on the interior state,
+// differentiated (the same formulas as below on complex scalars; pow as
+// exp(y log x) on the principal branch).  Dirichlet and vortex ghosts do not
+// depend on the state.
+template <int GAS>
+__device__ __forceinline__ bool bc_ghost2_exact(const BcDev& b, const GasParams& g, double nx, double ny,
+                                                const cplx in[4], cplx o[4])
+{
+    switch (b.kind)
+    {
+        case FRSDG_BC_SLIP_WALL:
+        {
+            const cplx u_in = in[1] / in[0], v_in = in[2] / in[0];
+            const cplx vn = u_in * nx + v_in * ny;
+            o[0] = in[0];
+            o[1] = in[0] * (u_in - 2.0 * vn * nx);
+            o[2] = in[0] * (v_in - 2.0 * vn * ny);
+            o[3] = in[3];
+            return true;
+        }
+        case FRSDG_BC_SUBSONIC_INFLOW:
+        {
+            const double gm = g.gamma;
+            const double p0 = b.params[0], T0 = b.params[1], Rg = b.params[2], ang = b.params[3];
+            const cplx rho_w = s_wrap_positive(in[0]);
+            const cplx E_w = s_wrap_positive(in[3]);
+            const cplx uu = in[1] / rho_w, vv = in[2] / rho_w;
+            const cplx e = E_w / rho_w - 0.5 * (uu * uu + vv * vv);
+            cplx p = gas_pressure<GAS>(g, rho_w, e);
+            if (p.re > p0) p = cplx(p0);
+            const cplx M2 = (2.0 / (gm - 1.0)) * (s_exp(((gm - 1.0) / gm) * s_log(cplx(p0) / p)) - 1.0);
+            const cplx T = cplx(T0) / (1.0 + 0.5 * (gm - 1.0) * M2);
+            const cplx rho = p / (Rg * T);
+            const cplx c = s_sqrt(gm * p / rho);
+            const cplx vel = s_sqrt(M2) * c;
+            const cplx u = vel * cos(ang), v = vel * sin(ang);
+            o[0] = rho;
+            o[1] = rho * u;
+            o[2] = rho * v;
+            o[3] = p / (gm - 1.0) + 0.5 * rho * (u * u + v * v);
+            return true;
+        }
+        case FRSDG_BC_PRESSURE_OUTLET:
+        {
+            const cplx rho = in[0];
+            const cplx u = in[1] / rho, v = in[2] / rho;
+            const cplx vel2 = s_sqrt(u * u + v * v) * s_sqrt(u * u + v * v);
+            const double pres = b.params[0];
+            o[0] = in[0];
+            o[1] = in[1];
+            o[2] = in[2];
+            if constexpr (GAS == FRSDG_GAS_IDEAL)
+                o[3] = pres / (g.gamma - 1.0) + 0.5 * rho * vel2;
+            else
+            {
+                const cplx covol = 1.0 - g.b * rho;
+                const cplx arho2 = g.a * rho * rho;
+                o[3] = ((pres + arho2) * covol) / (g.gamma - 1.0) - arho2 + 0.5 * rho * vel2;
+            }
+            return true;
+        }
+        default: return false;
+    }
+}
+
 // Ghost state of a 2D boundary face point (BoundaryConditions<T,2>::evaluate_bc,
 // boundary_conditions.hpp:239-248).  Native kinds act on the full scalar; the
-// other kinds stand for user lambdas and see only the real part (276-293).
+// other kinds stand for user lambdas and see only the real part (276-293),
+// unless `exact` asks for their complex-step derivative.
 template <int GAS, class S>
 __device__ __forceinline__ void bc_ghost2(const BcDev& b, int dir, const GasParams& g, double t, double x, double y, double nx, double ny, double Lx,
-                                          double Ly, const S in[4], S out[4])
+                                          double Ly, const S in[4], S out[4], bool exact = false)
 {
+    if constexpr (scalar_traits<S>::words == 2)
+    {
+        if (exact && bc_ghost2_exact<GAS>(b, g, nx, ny, in, out)) return;
+    }
     switch (b.kind)
     {
         case FRSDG_BC_OUTFLOW:

@@ -109,8 +109,23 @@ template <> struct NodeLoader<cplx>
     {
         const double2 x0 = __ldg(reinterpret_cast<const double2*>(a.U + off));
         const double2 x1 = __ldg(reinterpret_cast<const double2*>(a.U + off + 2));
-        const double2 v0 = __ldg(reinterpret_cast<const double2*>(a.W + off));
-        const double2 v1 = __ldg(reinterpret_cast<const double2*>(a.W + off + 2));
+        double2 v0, v1;
+        if (a.mode == MODE_JAC)
+        {
+            // seed of this launch slice: DOF d of every element of colour c
+            const int64_t eg = off / a.nd;
+            const int d0 = int(off - eg * a.nd);
+            const int gi = int(eg % a.Nx), gj = int(eg / a.Nx);
+            const int c = int(blockIdx.z) / a.nd, d = int(blockIdx.z) - c * a.nd;
+            const bool on = elem_colour(a.jac_cmode, a.Nx, a.Ny, a.per_x, a.per_y, gi, gj) == c;
+            v0 = make_double2(on && d == d0 ? 1.0 : 0.0, on && d == d0 + 1 ? 1.0 : 0.0);
+            v1 = make_double2(on && d == d0 + 2 ? 1.0 : 0.0, on && d == d0 + 3 ? 1.0 : 0.0);
+        }
+        else
+        {
+            v0 = __ldg(reinterpret_cast<const double2*>(a.W + off));
+            v1 = __ldg(reinterpret_cast<const double2*>(a.W + off + 2));
+        }
         s[0] = cplx(x0.x, v0.x * a.h);
         s[1] = cplx(x0.y, v0.y * a.h);
         s[2] = cplx(x1.x, v1.x * a.h);
@@ -150,7 +165,7 @@ __device__ __noinline__ Rec<S> ghost_record(const Fr2dArgs& a, int dir, int64_t 
 {
     S s_in[4], s_out[4];
     NodeLoader<S>::load(a, interior_off, s_in);
-    bc_ghost2<GAS>(a.bc[dir], dir, a.gas, a.t, x, y, nx, ny, a.Lx, a.Ly, s_in, s_out);
+    bc_ghost2<GAS>(a.bc[dir], dir, a.gas, a.t, x, y, nx, ny, a.Lx, a.Ly, s_in, s_out, a.exact_bc != 0);
     const NodePrim<S> pr = node_prim<GAS>(a.gas, s_out[0], s_out[1], s_out[2], s_out[3]);
     Rec<S> out;
     make_record<GAS>(a.gas, s_out, pr, out.v);
@@ -508,6 +523,10 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
         const S* dyb = sDel + ((e * 4 + 2) * 4 + eq) * N;
         const S* dyt = sDel + ((e * 4 + 3) * 4 + eq) * N;
         const int64_t gbase = (int64_t(j0 + ty) * Nx + (i0 + tx)) * ND + eq;
+        // coloured Jacobian: this slice's column d of the blocks of colour-c elements
+        const int jz = int(blockIdx.z), jc = jz / ND, jd = jz % ND;
+        const bool jac_store = a.mode == MODE_JAC &&
+                               elem_colour(a.jac_cmode, Nx, Ny, a.per_x, a.per_y, i0 + tx, j0 + ty) == jc;
         S gr[N];
         if constexpr (GEO == GEO_CURVED)
         {
@@ -546,7 +565,9 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
             {
                 double jv = a.sigma * sSeed[(e * 4 + eq) * NN + l * N + k] * a.inv_h;
                 jv += s_im(R) * a.inv_h;
-                out[gidx] = jv;
+                if (a.mode != MODE_JAC) out[gidx] = jv;
+                else if (jac_store)
+                    out[(int64_t(j0 + ty) * Nx + (i0 + tx)) * int64_t(ND * ND) + int64_t(jd) * ND + (l * N + k) * 4 + eq] = jv;
             }
             else
             {
@@ -570,7 +591,8 @@ cudaError_t launch_fr2d_kernel(const Fr2dArgs& a, cudaStream_t st)
         if (e != cudaSuccess) return e;
         attr_done = true;
     }
-    dim3 grid((a.Nx + T::TX - 1) / T::TX, (a.Ny + T::TY - 1) / T::TY);
+    dim3 grid((a.Nx + T::TX - 1) / T::TX, (a.Ny + T::TY - 1) / T::TY,
+              a.mode == MODE_JAC ? (a.jac_cmode ? 9 : 2) * T::NN * 4 : 1);
     kern<<<grid, T::BT, T::bytes, st>>>(a);
     return cudaGetLastError();
 }

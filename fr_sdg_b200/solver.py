@@ -35,6 +35,7 @@ class FRSolver:
         n = C.c_int64()
         A.check(self._lib.frsdg_n_dofs(h, C.byref(n)), "frsdg_n_dofs")
         self.n_dofs = int(n.value)
+        self.n_elems = cfg.n_elems[0] * (cfg.n_elems[1] if cfg.dim == 2 else 1)
 
     # -- lifetime ---------------------------------------------------------
     def close(self) -> None:
@@ -89,6 +90,25 @@ class FRSolver:
     def matmult(self, v: torch.Tensor, out: torch.Tensor) -> None:
         self._check_vec(v, out)
         A.check(self._lib.frsdg_jvp(self._h, _ptr(v), _ptr(out), _stream()), "frsdg_jvp")
+
+    def jac_blocks(self, t: float, sigma: float, U: torch.Tensor, blocks: torch.Tensor) -> None:
+        """Element-diagonal Jacobian blocks (coloured complex step), blocks[e] column-major."""
+        self._check_vec(U)
+        nd = self.n_dofs // self.n_elems
+        if blocks.dtype != torch.float64 or not blocks.is_cuda or not blocks.is_contiguous() \
+                or blocks.numel() != self.n_elems * nd * nd:
+            raise ValueError(f"expected a contiguous float64 CUDA tensor of {self.n_elems * nd * nd} entries")
+        A.check(self._lib.frsdg_jac_blocks(self._h, t, sigma, _ptr(U), _ptr(blocks), _stream()), "frsdg_jac_blocks")
+
+    def pc_setup(self, t: float, sigma: float, U: torch.Tensor) -> None:
+        """Block-Jacobi preconditioner at (t, sigma, U): blocks and their FP32 inverses."""
+        self._check_vec(U)
+        A.check(self._lib.frsdg_pc_setup(self._h, t, sigma, _ptr(U), _stream()), "frsdg_pc_setup")
+
+    def pc_apply(self, r: torch.Tensor, z: torch.Tensor) -> None:
+        """z = inv(block diagonal) r."""
+        self._check_vec(r, z)
+        A.check(self._lib.frsdg_pc_apply(self._h, _ptr(r), _ptr(z), _stream()), "frsdg_pc_apply")
 
     def apply_stabilization(self, U: torch.Tensor) -> None:
         self._check_vec(U)

@@ -124,7 +124,11 @@ typedef struct frsdg_config {
     double  shock_theta;     /* default 1 */
     double  shock_threshold; /* default 0.8 */
     int32_t cond_sys;        /* -solve_positive_preserving: unknowns (log rho, u, [v], log e) */
-    int32_t pad1_;
+    int32_t jvp_exact_bc;    /* 0 (default): the complex-step JVP and Jacobian blocks see the
+                                boundary ghosts of user-lambda boundary kinds (slip wall, Dirichlet,
+                                vortex, subsonic inflow, pressure outlet) as constants, as the
+                                reference does (boundary_conditions.hpp:276-293); 1: they are
+                                differentiated too (exact Jacobian; 2D only) */
     double  csd_eps;         /* complex-step h (reference: 1e-7, petsc_solver_impl.hpp:179) */
 } frsdg_config;
 
@@ -168,6 +172,27 @@ int frsdg_jvp_prepare(frsdg_handle* h, double t, double sigma, const double* U);
 /* JV = sigma*Im(M(U+ihV))/h + Im(R(M(U+ihV)))/h, h = cfg.csd_eps:
  * ComplexStepJacobianStrategy::matmult (petsc_solver_impl.hpp:250-432). */
 int frsdg_jvp(frsdg_handle* h, const double* V, double* JV, void* stream);
+
+/* Element-diagonal blocks of the implicit Jacobian J = sigma*dM/dU + dR(M(U))/dU at
+ * (t, U), by complex step (h = cfg.csd_eps) with element colouring, in one launch:
+ * the preconditioner's part of ComplexStepJacobianStrategy::pre_jv_eval
+ * (petsc_solver_impl.hpp:223-248), which assembles its preconditioner by DMDA-coloured
+ * finite differences (MatFDColoringApply, 72-95, 244).  Elements of one colour share
+ * no face, so seeding DOF d of every element of colour c gives column d of each such
+ * element's block.  blocks: nelem * nd * nd doubles (nd = 4 (p+1)^2), block e
+ * column-major: blocks[(e*nd + col)*nd + row].  2D only. */
+int frsdg_jac_blocks(frsdg_handle* h, double t, double sigma, const double* U,
+                     double* blocks, void* stream);
+
+/* Block-Jacobi preconditioner for the Newton-Krylov solve (the PCSetUp / PCApply
+ * pair PETSc runs on the coloured Jacobian): frsdg_pc_setup computes the blocks of
+ * frsdg_jac_blocks into handle-owned storage (allocated by the first call:
+ * nelem*nd*nd doubles and as many floats), inverts each block in FP64 with partial
+ * pivoting, keeps the inverses in FP32, synchronises the stream and fails with
+ * FRSDG_ERR_ARG on a zero pivot; p <= 5.  frsdg_pc_apply: z_e = inv(J_ee) r_e for
+ * every element (z must not alias r). */
+int frsdg_pc_setup(frsdg_handle* h, double t, double sigma, const double* U, void* stream);
+int frsdg_pc_apply(frsdg_handle* h, const double* r, double* z, void* stream);
 
 /* One explicit Runge-Kutta stage fused into the residual pass:
  *   out = alpha*A + beta*B + gamma*rhs(Us),   acc += delta*rhs(Us)   (rhs = -R)
