@@ -23,6 +23,8 @@ import sys
 import time
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
@@ -306,13 +308,35 @@ def run_ours(args, ws, rank, local):
             vint = Integrator(vs, "rk4")
             vint.step(V, 0.0, vdt)
             V.copy_(vw.init(f"cuda:{local}"))
-            vst, vms = timed(lambda: vint.run(V, vdt, t_end=vw.t_end))
+            vst, vms = timed(lambda: vint.run(V, vdt, t_end=vw.t_end, graph=True))
             x, y = node_coords(vw.cfg, f"cuda:{local}")
             err = l2_error(vw.cfg, V, pack2d(*exact_vortex(vst.t, x, y)), node_jacobian(vw.cfg, V.device))
             vortex = {"workload": vw.name, "seconds": vms / 1e3, "steps": vst.steps, "t_end": vst.t, "dt": vdt,
-                      "scheme": "RK4", "l2_density_error_vs_exact": float(err[0]),
+                      "scheme": "RK4, CUDA graphs of 64 steps", "l2_density_error_vs_exact": float(err[0]),
                       "finite": vs.status() == 0}
-        t_end = {"vortex_curved_64x64_p4": vortex, "blast_200_steps": blast}
+        # (3) The 1D Sod tube (200 elements, p = 3, SSP-RK3 + WENO, t = 0.2): launch-latency
+        # bound, so the full steps replay CUDA graphs; L1 density error against the exact
+        # Riemann solution (Toro, ch. 4).
+        from fr_sdg_b200 import refelem
+        from fr_sdg_b200.exact_riemann import sod_exact
+        from fr_sdg_b200.workloads import sod1d
+        sw = sod1d()
+        with FRSolver(sw.cfg) as ss:
+            S = sw.init(f"cuda:{local}")
+            sdt = cfl_time_step(sw.cfg, S, sw.cfl)
+            sint = Integrator(ss, "ssprk3")
+            sint.step(S, 0.0, sdt)
+            S.copy_(sw.init(f"cuda:{local}"))
+            sst, sms = timed(lambda: sint.run(S, sdt, t_end=sw.t_end, graph=True))
+            xs, _ = node_coords(sw.cfg, "cpu")
+            n1 = sw.cfg.poly_deg + 1
+            rho = S.view(-1, 3, n1)[:, 0].cpu().numpy()
+            w1 = np.array(refelem.reference_element(sw.cfg.poly_deg)[1]) * 0.5 / sw.cfg.n_elems[0]
+            l1 = float(np.sum(w1[None, :] * np.abs(rho - sod_exact(xs.numpy(), sst.t))))
+            sod = {"workload": sw.name, "seconds": sms / 1e3, "steps": sst.steps, "t_end": sst.t, "dt": sdt,
+                   "scheme": "SSP-RK3 + WENO/shock sensor, CUDA graphs of 64 steps",
+                   "l1_density_error_vs_exact": l1, "finite": ss.status() == 0}
+        t_end = {"vortex_curved_64x64_p4": vortex, "blast_200_steps": blast, "sod1d_200_p3": sod}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

@@ -1,7 +1,7 @@
-"""Exact solution of the Sod shock tube (ideal gas, gamma = 1.4) for the tests:
+"""Exact solution of the Sod shock tube (ideal gas, gamma = 1.4):
 the classical two-rarefaction/shock Riemann solution with Newton iteration on the
 star pressure (E. F. Toro, "Riemann Solvers and Numerical Methods for Fluid
-Dynamics", ch. 4).  Test support only."""
+Dynamics", ch. 4), for error measurements of shock-tube runs."""
 from __future__ import annotations
 
 import math

@@ -11,7 +11,7 @@ from fr_sdg_b200.integrate import Integrator, cfl_time_step, l2_error, node_jaco
 from fr_sdg_b200.workloads import blast_large, exact_vortex, node_coords, pack2d, sod1d, vortex_curved
 from oracle.oracle import Oracle
 from tests.helpers import rel_err
-from tests.sod_exact import sod_exact
+from fr_sdg_b200.exact_riemann import sod_exact
 
 pytestmark = pytest.mark.gpu
 
@@ -104,3 +104,22 @@ def test_sod_against_exact_riemann(cuda):
     w = np.array([1 / 6, 5 / 6, 5 / 6, 1 / 6]) * 0.5 * (1.0 / 200)
     l1 = float(np.sum(w[None, :] * np.abs(rho - rho_ex)))
     assert l1 < 5e-3, f"L1 density error {l1:.3e}"
+
+
+@pytest.mark.parametrize("name", ["vortex_rk4", "sod1d_weno"])
+def test_graph_replay_matches_eager(name, cuda):
+    """The CUDA-graph replay of full steps gives the eager run's state bit for bit."""
+    if name == "vortex_rk4":
+        wl, scheme = vortex_curved(n_elems=12, p=4), "rk4"
+    else:
+        wl, scheme = sod1d(), "ssprk3"
+    with FRSolver(wl.cfg) as s:
+        U0 = wl.init(cuda)
+        dt = cfl_time_step(wl.cfg, U0, wl.cfl)
+        Ue, Ug = U0.clone(), U0.clone()
+        t_end = 25.5 * dt
+        se = Integrator(s, scheme).run(Ue, dt, t_end=t_end)
+        sg = Integrator(s, scheme).run(Ug, dt, t_end=t_end, graph=True, steps_per_graph=8)
+        assert se.steps == sg.steps == 26 and abs(sg.t - t_end) < 1e-15 and sg.t == se.t
+        assert torch.equal(Ue, Ug)
+        assert s.status() == 0
