@@ -228,6 +228,28 @@ def run_ours(args, ws, rank, local):
     value = ws * dofs * args.steps / (elapsed_ms / 1e3)
     bad = solver.status()
 
+    # ---- the same residual in FP32 (mixed-precision form), device-resident
+    mixed = None
+    if not args.no_t_end:
+        U32 = U.float()
+        F32 = torch.empty_like(U32)
+        for _ in range(3):
+            solver.residual_kernel_f32(0.0, U32, F32)
+        barrier()
+        torch.cuda.synchronize()
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        for _ in range(args.steps):
+            solver.residual_kernel_f32(0.0, U32, F32)
+        m1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        mms = m0.elapsed_time(m1) / args.steps
+        mixed = {"fp32_residual_ms": mms, "fp32_dof_residuals_per_s": ws * dofs / (mms / 1e3),
+                 "speedup_vs_fp64": (elapsed_ms / args.steps) / mms}
+        del U32, F32
+
     # ---- end to end through the host-buffer entry point
     e2e = None
     if not args.no_e2e:
@@ -336,7 +358,19 @@ def run_ours(args, ws, rank, local):
             sod = {"workload": sw.name, "seconds": sms / 1e3, "steps": sst.steps, "t_end": sst.t, "dt": sdt,
                    "scheme": "SSP-RK3 + WENO/shock sensor, CUDA graphs of 64 steps",
                    "l1_density_error_vs_exact": l1, "finite": ss.status() == 0}
-        t_end = {"vortex_curved_64x64_p4": vortex, "blast_200_steps": blast, "sod1d_200_p3": sod}
+        # (4) The vortex again in mixed precision (FP32 residuals, FP64 stage sums)
+        with FRSolver(vw.cfg) as vs:
+            V = vw.init(f"cuda:{local}")
+            vint = Integrator(vs, "rk4", mixed=True)
+            vint.step(V, 0.0, vdt)
+            V.copy_(vw.init(f"cuda:{local}"))
+            mst, mms2 = timed(lambda: vint.run(V, vdt, t_end=vw.t_end, graph=True))
+            merr = l2_error(vw.cfg, V, pack2d(*exact_vortex(mst.t, x, y)), node_jacobian(vw.cfg, V.device))
+            vortex_mixed = {"workload": vw.name, "seconds": mms2 / 1e3, "steps": mst.steps, "t_end": mst.t,
+                            "scheme": "RK4 mixed (FP32 residual, FP64 stages), CUDA graphs of 64 steps",
+                            "l2_density_error_vs_exact": float(merr[0]), "finite": vs.status() == 0}
+        t_end = {"vortex_curved_64x64_p4": vortex, "vortex_curved_64x64_p4_mixed": vortex_mixed,
+                 "blast_200_steps": blast, "sod1d_200_p3": sod}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -365,7 +399,7 @@ def run_ours(args, ws, rank, local):
                    "l2": f"inputs ({dofs * 8 / 1e9:.2f} GB) larger than L2 (126 MB); no flush",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
         "clocks": clk.summary(), "gpu_launches": args.steps, "roofline": roof, "e2e": e2e,
-        "cpu_baseline": cpu, "bad_density_nodes": bad, "time_to_t_end": t_end,
+        "cpu_baseline": cpu, "bad_density_nodes": bad, "time_to_t_end": t_end, "mixed_precision": mixed,
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -31,6 +31,9 @@ namespace frsdg
     FRSDG_DECL(S, 8) FRSDG_DECL(S, 9) FRSDG_DECL(S, 10)
 FRSDG_DECL_ALL(double)
 FRSDG_DECL_ALL(cplx)
+#define FRSDG_DECL2(S, N) extern template cudaError_t launch_fr2d<S, N>(int, int, int, const Fr2dArgs&, cudaStream_t);
+FRSDG_DECL2(float, 2) FRSDG_DECL2(float, 3) FRSDG_DECL2(float, 4) FRSDG_DECL2(float, 5) FRSDG_DECL2(float, 6)
+FRSDG_DECL2(float, 7) FRSDG_DECL2(float, 8) FRSDG_DECL2(float, 9) FRSDG_DECL2(float, 10)
 } // namespace frsdg
 
 namespace
@@ -285,6 +288,8 @@ int frsdg_create(const frsdg_config* cfg, frsdg_handle** out)
     Ops ops{};
     for (int q = 0; q < n * n; ++q) ops.D[q] = h->re.D[q];
     for (int q = 0; q < n; ++q) { ops.dL[q] = h->re.dL[q]; ops.dR[q] = h->re.dR[q]; ops.csi[q] = h->re.x[q]; }
+    for (int q = 0; q < n * n; ++q) ops.Df[q] = static_cast<float>(ops.D[q]);
+    for (int q = 0; q < n; ++q) { ops.dLf[q] = static_cast<float>(ops.dL[q]); ops.dRf[q] = static_cast<float>(ops.dR[q]); }
     const GasParams gas{cfg->gamma, cfg->gas_law == FRSDG_GAS_VDW ? cfg->vdw_a : 0.0,
                         cfg->gas_law == FRSDG_GAS_VDW ? cfg->vdw_b : 0.0};
     const bool per_x = cfg->bc[FRSDG_LEFT].kind == FRSDG_BC_PERIODIC;
@@ -584,6 +589,46 @@ int frsdg_jvp(frsdg_handle* h, const double* V, double* JV, void* stream)
     if (!h->jvp_U) return fail(FRSDG_ERR_ARG, "frsdg_jvp called before frsdg_jvp_prepare");
     if (reinterpret_cast<uintptr_t>(V) & 15) return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
     return run_residual(h, MODE_JVP, h->jvp_t, h->jvp_U, V, JV, stream);
+}
+
+// Residual pass of the FP32 instantiation (2D): U32 is a float state, out is
+// float (out_f32) or double (the stage forms).
+static int run_residual_f32(frsdg_handle* h, int mode, double t, const float* U32, void* out, bool out_f32,
+                            const StageArgs* stage, void* stream)
+{
+    if (h->cfg.dim != 2) return fail(FRSDG_ERR_UNSUPPORTED, "FP32 residual: 2D configurations only");
+    if ((reinterpret_cast<uintptr_t>(U32) | reinterpret_cast<uintptr_t>(out)) & 15)
+        return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    h->last = s;
+    Fr2dArgs a = h->a2;
+    a.t = t;
+    a.mode = mode;
+    a.cond_sys = 0;
+    a.U = reinterpret_cast<const double*>(U32);
+    a.W = nullptr;
+    a.out = out;
+    a.out_f32 = out_f32 ? 1 : 0;
+    if (stage) a.st = *stage;
+    const cudaError_t e = dispatch2d<float>(h->n, h->cfg.gas_law, h->cfg.riemann, h->geo, a, s);
+    if (e != cudaSuccess) return cuda_fail(e, "FP32 residual launch");
+    return FRSDG_OK;
+}
+
+int frsdg_residual_f32(frsdg_handle* h, double t, const float* U32, float* R32, void* stream)
+{
+    if (!h || !U32 || !R32) return fail(FRSDG_ERR_ARG, "null argument");
+    return run_residual_f32(h, MODE_RESIDUAL, t, U32, R32, true, nullptr, stream);
+}
+
+int frsdg_rk_stage_mixed(frsdg_handle* h, double t, const float* Us32, const double* A, double alpha, const double* B,
+                         double beta, double gamma, double* out, float* out32, double* acc, double delta, void* stream)
+{
+    if (!h || !Us32 || !out) return fail(FRSDG_ERR_ARG, "null argument");
+    if (reinterpret_cast<const void*>(out32) == reinterpret_cast<const void*>(Us32))
+        return fail(FRSDG_ERR_ARG, "frsdg_rk_stage_mixed: out32 must not alias Us32");
+    StageArgs st{A, B, acc, alpha, beta, gamma, delta, out32};
+    return run_residual_f32(h, MODE_STAGE, t, Us32, out, false, &st, stream);
 }
 
 int frsdg_jac_blocks(frsdg_handle* h, double t, double sigma, const double* U, double* blocks, void* stream)

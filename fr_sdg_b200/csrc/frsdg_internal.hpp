@@ -29,6 +29,7 @@ struct StageArgs
     const double* B;   // may be null
     double*       acc; // may be null
     double alpha, beta, gamma, delta;
+    float*        out32; // may be null: FP32 copy of out (the next stage's input in mixed precision)
 };
 
 // Geometry classes of the 2D kernel: constant diagonal metrics (Cartesian and the
@@ -54,7 +55,21 @@ struct Ops
     double dL[kMaxN];
     double dR[kMaxN];
     double csi[kMaxN];
+    float  Df[kMaxN * kMaxN];  // FP32 copies for the single-precision residual
+    float  dLf[kMaxN];
+    float  dRf[kMaxN];
 };
+
+// Operator entries in the arithmetic type T of a residual instantiation.
+template <class T> __device__ __forceinline__ T opD(const Ops& o, int i);
+template <> __device__ __forceinline__ double opD<double>(const Ops& o, int i) { return o.D[i]; }
+template <> __device__ __forceinline__ float opD<float>(const Ops& o, int i) { return o.Df[i]; }
+template <class T> __device__ __forceinline__ T opL(const Ops& o, int i);
+template <> __device__ __forceinline__ double opL<double>(const Ops& o, int i) { return o.dL[i]; }
+template <> __device__ __forceinline__ float opL<float>(const Ops& o, int i) { return o.dLf[i]; }
+template <class T> __device__ __forceinline__ T opR(const Ops& o, int i);
+template <> __device__ __forceinline__ double opR<double>(const Ops& o, int i) { return o.dR[i]; }
+template <> __device__ __forceinline__ float opR<float>(const Ops& o, int i) { return o.dRf[i]; }
 
 struct GasParams
 {
@@ -81,6 +96,7 @@ struct Fr2dArgs
     unsigned long long* bad;
     StageArgs st;
     int    nd;         // DOFs per element, 4 n^2
+    int    out_f32;    // residual written as float (FP32 instantiation)
     int    exact_bc;   // complex scalars: differentiate the user-lambda boundary kinds too
     int    jac_cmode;  // MODE_JAC colouring: 0 checkerboard, 1 three-colour cycles (odd periodic)
     Ops    ops;
@@ -151,7 +167,9 @@ __device__ __forceinline__ void store_residual(int mode, const double* W, const 
         double o = 0.0;
         if (st.A) o = st.alpha * __ldg(st.A + idx);
         if (st.B) o = o + st.beta * __ldg(st.B + idx);
-        out[idx] = o + st.gamma * v;
+        const double ov = o + st.gamma * v;
+        out[idx] = ov;
+        if (st.out32) st.out32[idx] = static_cast<float>(ov);
         if (st.acc) st.acc[idx] = st.acc[idx] + st.delta * v;
     }
     else out[idx] = r;

@@ -103,6 +103,23 @@ template <> struct NodeLoader<double>
     }
 };
 
+template <> struct NodeLoader<float>
+{
+    __device__ static void load(const Fr2dArgs& a, int64_t off, float s[4])
+    {
+        const float4 x = __ldg(reinterpret_cast<const float4*>(reinterpret_cast<const float*>(a.U) + off));
+        s[0] = x.x; s[1] = x.y; s[2] = x.z; s[3] = x.w;
+        if (a.cond_sys)
+        {
+            const float rho  = expf(s[0]);
+            const float ssq  = (0.0f + s[1] * s[1]) + s[2] * s[2];
+            const float rhoE = rho * (expf(s[3]) + 0.5f * ssq);
+            const float u = s[1], v = s[2];
+            s[0] = rho; s[1] = rho * u; s[2] = rho * v; s[3] = rhoE;
+        }
+    }
+};
+
 template <> struct NodeLoader<cplx>
 {
     __device__ static void load(const Fr2dArgs& a, int64_t off, cplx s[4])
@@ -282,6 +299,7 @@ __device__ __forceinline__ void face_jumps(const Fr2dArgs& a, int i0, int j0, bo
                                            const S Fs[4], const S* sF, const S* sG, S* sDel)
 {
     constexpr int TX = tile_x(N), NN = N * N;
+    using R_t = typename scalar_traits<S>::real;
     if (!valid) return;
 #pragma unroll
     for (int side = 0; side < 2; ++side)
@@ -305,10 +323,10 @@ __device__ __forceinline__ void face_jumps(const Fr2dArgs& a, int i0, int j0, bo
         {
             S fn;
             if constexpr (GEO == GEO_CURVED)
-                fn = sF[(e * 4 + eq) * NN + node] * sd[side].nx + sG[(e * 4 + eq) * NN + node] * sd[side].ny;
+                fn = sF[(e * 4 + eq) * NN + node] * R_t(sd[side].nx) + sG[(e * 4 + eq) * NN + node] * R_t(sd[side].ny);
             else
                 fn = XF ? sF[(e * 4 + eq) * NN + node] : sG[(e * 4 + eq) * NN + node];
-            sDel[((e * 4 + sdi) * 4 + eq) * N + pos] = sc * (Fs[eq] - fn);
+            sDel[((e * 4 + sdi) * 4 + eq) * N + pos] = R_t(sc) * (Fs[eq] - fn);
         }
     }
 }
@@ -319,6 +337,7 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
 {
     using T = Tile2D<S, N, GEO>;
     constexpr int TX = T::TX, TY = T::TY, NN = T::NN, TE = T::TE, BT = T::BT, NREC = T::NREC;
+    using R_t = typename scalar_traits<S>::real;
     constexpr int ND = 4 * NN;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     S* sm   = reinterpret_cast<S*>(smem_raw);
@@ -485,11 +504,11 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
 #pragma unroll
                     for (int m = 0; m < N; ++m)
                     {
-                        dG = dG + a.ops.D[l * N + m] * gv[m];
-                        dF = dF + a.ops.D[l * N + m] * fv[m];
+                        dG = dG + opD<R_t>(a.ops, l * N + m) * gv[m];
+                        dF = dF + opD<R_t>(a.ops, l * N + m) * fv[m];
                     }
                     const double2 me = __ldg(reinterpret_cast<const double2*>(mt + l * N * 4));
-                    sC[(e * 4 + eq) * NN + l * N + k] = me.x * dF + me.y * dG;
+                    sC[(e * 4 + eq) * NN + l * N + k] = R_t(me.x) * dF + R_t(me.y) * dG;
                 }
             }
             else
@@ -499,8 +518,8 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
                 {
                     S dG = S(0.0);
 #pragma unroll
-                    for (int m = 0; m < N; ++m) dG = dG + a.ops.D[l * N + m] * gv[m];
-                    sC[(e * 4 + eq) * NN + l * N + k] = a.eta_y * dG;
+                    for (int m = 0; m < N; ++m) dG = dG + opD<R_t>(a.ops, l * N + m) * gv[m];
+                    sC[(e * 4 + eq) * NN + l * N + k] = R_t(a.eta_y) * dG;
                 }
             }
         }
@@ -517,7 +536,7 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
         S fv[N];
 #pragma unroll
         for (int m = 0; m < N; ++m) fv[m] = Fr[m];
-        const double dLl = a.ops.dL[l], dRl = a.ops.dR[l];
+        const R_t dLl = opL<R_t>(a.ops, l), dRl = opR<R_t>(a.ops, l);
         const S dxl = sDel[((e * 4 + 0) * 4 + eq) * N + l];
         const S dxr = sDel[((e * 4 + 1) * 4 + eq) * N + l];
         const S* dyb = sDel + ((e * 4 + 2) * 4 + eq) * N;
@@ -539,24 +558,24 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
         {
             S dF = S(0.0);
 #pragma unroll
-            for (int m = 0; m < N; ++m) dF = dF + a.ops.D[k * N + m] * fv[m];
+            for (int m = 0; m < N; ++m) dF = dF + opD<R_t>(a.ops, k * N + m) * fv[m];
             S R;
             if constexpr (GEO == GEO_CURVED)
             {
                 S dG = S(0.0);
 #pragma unroll
-                for (int m = 0; m < N; ++m) dG = dG + a.ops.D[k * N + m] * gr[m];
+                for (int m = 0; m < N; ++m) dG = dG + opD<R_t>(a.ops, k * N + m) * gr[m];
                 const double2 mx = __ldg(reinterpret_cast<const double2*>(
                     a.metrics + ((int64_t(j0 + ty) * Nx + (i0 + tx)) * NN + l * N + k) * 4));
-                R = (mx.x * dF + mx.y * dG) + sC[(e * 4 + eq) * NN + l * N + k];
+                R = (R_t(mx.x) * dF + R_t(mx.y) * dG) + sC[(e * 4 + eq) * NN + l * N + k];
             }
             else
             {
-                const S px = a.xi_x * dF;
+                const S px = R_t(a.xi_x) * dF;
                 R = px + sC[(e * 4 + eq) * NN + l * N + k];
             }
-            R = R + dxl * a.ops.dL[k];
-            R = R + dxr * a.ops.dR[k];
+            R = R + dxl * opL<R_t>(a.ops, k);
+            R = R + dxr * opR<R_t>(a.ops, k);
             R = R + dyb[k] * dLl;
             R = R + dyt[k] * dRl;
             const int64_t gidx = gbase + (l * N + k) * 4;
@@ -569,6 +588,8 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
                 else if (jac_store)
                     out[(int64_t(j0 + ty) * Nx + (i0 + tx)) * int64_t(ND * ND) + int64_t(jd) * ND + (l * N + k) * 4 + eq] = jv;
             }
+            else if (a.out_f32)
+                reinterpret_cast<float*>(a.out)[gidx] = static_cast<float>(s_re(R));
             else
             {
                 store_residual(a.mode, a.W, a.st, out, gidx, s_re(R));

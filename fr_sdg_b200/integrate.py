@@ -62,13 +62,20 @@ class RunStats:
 
 
 class Integrator:
-    """SSP-RK3 / RK4 over one FRSolver; buffers are allocated once."""
+    """SSP-RK3 / RK4 over one FRSolver; buffers are allocated once.
 
-    def __init__(self, solver: FRSolver, scheme: str = "ssprk3"):
+    mixed=True: every stage takes the residual in FP32 from an FP32 copy of its input
+    (frsdg_rk_stage_mixed) and combines the stages in FP64; the FP64 state stays the
+    solution.  The FP32 copy of U is refreshed at the end of every step."""
+
+    def __init__(self, solver: FRSolver, scheme: str = "ssprk3", mixed: bool = False):
         if scheme not in ("ssprk3", "rk4"):
             raise ValueError("scheme must be 'ssprk3' or 'rk4'")
+        if mixed and (solver.cfg.dim != 2 or solver.cfg.cond_sys):
+            raise ValueError("mixed precision: 2D configurations without change of variables")
         self.s = solver
         self.scheme = scheme
+        self.mixed = mixed
         self._buf = None
         cfg = solver.cfg
         self.stabilise = bool(cfg.apply_filter or cfg.apply_weno)
@@ -76,12 +83,34 @@ class Integrator:
     def _buffers(self, U: torch.Tensor):
         if self._buf is None or self._buf[0].device != U.device:
             self._buf = [torch.empty_like(U) for _ in range(3)]
+            if self.mixed:
+                self._buf += [torch.empty(U.shape, dtype=torch.float32, device=U.device) for _ in range(3)]
         return self._buf
+
+    def _step_mixed(self, U: torch.Tensor, t: float, dt: float) -> None:
+        s = self.s
+        b1, b2, b3, u32, c1, c2 = self._buffers(U)
+        u32.copy_(U)
+        if self.scheme == "ssprk3":
+            s.rk_stage_mixed(t, u32, b1, c1, gamma=dt, a=U, alpha=1.0)
+            s.rk_stage_mixed(t + dt, c1, b2, c2, gamma=0.25 * dt, a=U, alpha=0.75, b=b1, beta=0.25)
+            s.rk_stage_mixed(t + 0.5 * dt, c2, U, None, gamma=2.0 * dt / 3.0, a=U, alpha=1.0 / 3.0, b=b2,
+                             beta=2.0 / 3.0)
+        else:
+            b3.copy_(U)
+            s.rk_stage_mixed(t, u32, b1, c1, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 6.0)
+            s.rk_stage_mixed(t + 0.5 * dt, c1, b2, c2, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
+            s.rk_stage_mixed(t + 0.5 * dt, c2, b1, c1, gamma=dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
+            s.rk_stage_mixed(t + dt, c1, U, None, gamma=dt / 6.0, a=b3, alpha=1.0)
+        if self.stabilise:
+            s.apply_stabilization(U)
 
     def step(self, U: torch.Tensor, t: float, dt: float) -> None:
         """Advance U (in place) from t to t + dt, then apply the post-step limiter."""
+        if self.mixed:
+            return self._step_mixed(U, t, dt)
         s = self.s
-        b1, b2, b3 = self._buffers(U)
+        b1, b2, b3 = self._buffers(U)[:3]
         if self.scheme == "ssprk3":
             s.rk_stage(t, U, b1, gamma=dt, a=U, alpha=1.0)
             s.rk_stage(t + dt, b1, b2, gamma=0.25 * dt, a=U, alpha=0.75, b=b1, beta=0.25)

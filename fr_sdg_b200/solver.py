@@ -82,6 +82,26 @@ class FRSolver:
         A.check(self._lib.frsdg_rk_stage(self._h, t, _ptr(Us), p(a), alpha, p(b), beta, gamma, _ptr(out),
                                          p(acc), delta, _stream()), "frsdg_rk_stage")
 
+    def _check_f32(self, *vs: torch.Tensor) -> None:
+        for v in vs:
+            if v.dtype != torch.float32 or not v.is_cuda or not v.is_contiguous() or v.numel() != self.n_dofs:
+                raise ValueError(f"expected a contiguous float32 CUDA vector of {self.n_dofs} entries")
+
+    def residual_kernel_f32(self, t: float, U32: torch.Tensor, R32: torch.Tensor) -> None:
+        """The residual in FP32 from an FP32 state (mixed-precision form)."""
+        self._check_f32(U32, R32)
+        A.check(self._lib.frsdg_residual_f32(self._h, t, _ptr(U32), _ptr(R32), _stream()), "frsdg_residual_f32")
+
+    def rk_stage_mixed(self, t: float, Us32: torch.Tensor, out: torch.Tensor, out32: torch.Tensor | None,
+                       gamma: float, a: torch.Tensor | None = None, alpha: float = 0.0, b: torch.Tensor | None = None,
+                       beta: float = 0.0, acc: torch.Tensor | None = None, delta: float = 0.0) -> None:
+        """out = alpha a + beta b + gamma rhs32(Us32) in FP64, out32 = float(out); acc += delta rhs."""
+        self._check_f32(Us32, *(v for v in (out32,) if v is not None))
+        self._check_vec(out, *(v for v in (a, b, acc) if v is not None))
+        p = lambda v: _ptr(v) if v is not None else None
+        A.check(self._lib.frsdg_rk_stage_mixed(self._h, t, _ptr(Us32), p(a), alpha, p(b), beta, gamma, _ptr(out),
+                                               p(out32), p(acc), delta, _stream()), "frsdg_rk_stage_mixed")
+
     def pre_jv_eval(self, t: float, U: torch.Tensor, sigma: float) -> None:
         self._check_vec(U)
         self._jvp_U = U  # keep alive while the library holds the pointer

@@ -173,6 +173,17 @@ int frsdg_jvp_prepare(frsdg_handle* h, double t, double sigma, const double* U);
  * ComplexStepJacobianStrategy::matmult (petsc_solver_impl.hpp:250-432). */
 int frsdg_jvp(frsdg_handle* h, const double* V, double* JV, void* stream);
 
+/* Mixed precision (2D; no reference counterpart -- the reference computes in FP64
+ * only).  frsdg_residual_f32: R = residual_kernel evaluated in FP32 on an FP32 state.
+ * frsdg_rk_stage_mixed: frsdg_rk_stage with the residual taken in FP32 from Us32 and the
+ * stage combination in FP64:
+ *   out = alpha*A + beta*B + gamma*rhs(Us32),  out32 = (float)out,  acc += delta*rhs
+ * (A, B, acc, out32 may be NULL; out32 must not alias Us32).  No change of variables. */
+int frsdg_residual_f32(frsdg_handle* h, double t, const float* U32, float* R32, void* stream);
+int frsdg_rk_stage_mixed(frsdg_handle* h, double t, const float* Us32, const double* A, double alpha,
+                         const double* B, double beta, double gamma, double* out, float* out32,
+                         double* acc, double delta, void* stream);
+
 /* Element-diagonal blocks of the implicit Jacobian J = sigma*dM/dU + dR(M(U))/dU at
  * (t, U), by complex step (h = cfg.csd_eps) with element colouring, in one launch:
  * the preconditioner's part of ComplexStepJacobianStrategy::pre_jv_eval

@@ -1,0 +1,87 @@
+"""GPU: the mixed-precision form -- the FP32 residual against the FP64 oracle on the
+same rounded state, the mixed RK stage (FP32 residual, FP64 combination), and
+whole vortex runs against their FP64 twins and the exact solution."""
+import numpy as np
+import pytest
+import torch
+
+from fr_sdg_b200 import FRSolver
+from fr_sdg_b200 import _abi as A
+from fr_sdg_b200.integrate import Integrator, cfl_time_step, l2_error, node_jacobian
+from fr_sdg_b200.workloads import exact_vortex, make_config, node_coords, pack2d, vortex_curved
+from oracle.oracle import Oracle
+from tests.helpers import TOL_FP32, random_state, rel_err
+
+pytestmark = pytest.mark.gpu
+
+PER = (A.BC_PERIODIC, None, None)
+OUT = A.BC_OUTFLOW
+CASES = {
+    "cart_ideal_hllc_p3": dict(p=3, n_elems=(7, 5), box=(1.3, 0.9), riemann="hllc",
+                               bcs={A.LEFT: OUT, A.RIGHT: OUT, A.TOP: A.BC_WALL, A.BOTTOM: OUT}),
+    "cart_vdw_rusanov_p5_periodic": dict(p=5, n_elems=(6, 4), riemann="rusanov", gas="vdw", vdw=(0.05, 0.02),
+                                         bcs={A.LEFT: PER, A.RIGHT: PER, A.TOP: PER, A.BOTTOM: PER}),
+    "sinewarp_hllc_p4_periodic": dict(p=4, n_elems=(6, 6), box=(10.0, 10.0), riemann="hllc",
+                                      geometry=A.GEOM_SINE_WARP, geom_params=(0.1, 0, 0, 0),
+                                      bcs={A.LEFT: PER, A.RIGHT: PER, A.TOP: PER, A.BOTTOM: PER}),
+    "bump_hllc_p3_inflow_outlet": dict(p=3, n_elems=(12, 4), box=(3.0, 0.8), riemann="hllc",
+                                       geometry=A.GEOM_WALL_PROFILE, profile=A.PROFILE_GAUSS_BUMP,
+                                       geom_params=(-1.5, 0.0625, 25.0, 0.0),
+                                       bcs={A.LEFT: (A.BC_SUBSONIC_INFLOW, None, (1.0, 1.0, 1.0, 0.0)),
+                                            A.RIGHT: (A.BC_PRESSURE_OUTLET, None, (0.84,)),
+                                            A.BOTTOM: A.BC_SLIP_WALL, A.TOP: A.BC_SLIP_WALL}),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_residual_f32_matches_oracle(name, cuda):
+    cfg = make_config(dim=2, **CASES[name])
+    U32 = random_state(cfg, 21, amp=0.3).astype(np.float32)
+    ref = Oracle(cfg, threads=4).residual(0.2, U32.astype(np.float64))
+    with FRSolver(cfg) as s:
+        Ud = torch.from_numpy(U32).to(cuda)
+        R = torch.empty_like(Ud)
+        s.residual_kernel_f32(0.2, Ud, R)
+        got = R.cpu().numpy()
+    err = rel_err(got, ref)
+    assert err <= TOL_FP32, f"{name}: FP32 residual rel err {err:.3e}"
+
+
+def test_rk_stage_mixed_combines_in_fp64(cuda):
+    cfg = make_config(dim=2, **CASES["sinewarp_hllc_p4_periodic"])
+    U = random_state(cfg, 3, amp=0.2)
+    U32 = U.astype(np.float32)
+    rng = np.random.default_rng(4)
+    Av, Bv, C0 = rng.uniform(-1, 1, U.size), rng.uniform(-1, 1, U.size), rng.uniform(-1, 1, U.size)
+    alpha, beta, gamma, delta = 0.75, 0.25, 0.013, 0.007
+    rhs = -Oracle(cfg, threads=4).residual(0.0, U32.astype(np.float64))
+    with FRSolver(cfg) as s:
+        d = lambda v: torch.from_numpy(np.ascontiguousarray(v)).to(cuda)
+        out, out32, acc = torch.empty(U.size, dtype=torch.float64, device=cuda), \
+            torch.empty(U.size, dtype=torch.float32, device=cuda), d(C0)
+        s.rk_stage_mixed(0.0, d(U32), out, out32, gamma=gamma, a=d(Av), alpha=alpha, b=d(Bv), beta=beta,
+                         acc=acc, delta=delta)
+        o, o32, ac = out.cpu().numpy(), out32.cpu().numpy(), acc.cpu().numpy()
+    ref = alpha * Av + beta * Bv + gamma * rhs
+    assert np.max(np.abs(o - ref)) <= TOL_FP32 * gamma * np.max(np.abs(rhs))
+    assert np.max(np.abs(ac - (C0 + delta * rhs))) <= TOL_FP32 * delta * np.max(np.abs(rhs))
+    assert np.array_equal(o32, o.astype(np.float32))
+
+
+@pytest.mark.parametrize("ne", [16, 32])
+def test_mixed_vortex_matches_fp64_accuracy(ne, cuda):
+    """Curved isentropic vortex, p = 4, RK4 to t = 1: the mixed-precision run's L2
+    density error against the exact solution is within 10 % of the FP64 run's."""
+    wl = vortex_curved(n_elems=ne, p=4)
+    errs = {}
+    with FRSolver(wl.cfg) as s:
+        x, y = node_coords(wl.cfg, cuda)
+        ex = pack2d(*exact_vortex(1.0, x, y))
+        J = node_jacobian(wl.cfg, cuda)
+        for mixed in (False, True):
+            U = wl.init(cuda)
+            dt = cfl_time_step(wl.cfg, U, 0.05)
+            Integrator(s, "rk4", mixed=mixed).run(U, dt, t_end=1.0)
+            errs[mixed] = float(l2_error(wl.cfg, U, ex, J)[0])
+        assert s.status() == 0
+    assert errs[True] <= 1.1 * errs[False], errs
