@@ -60,35 +60,62 @@ def traffic_per_launch():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 25 ms during the timed
+    region: the sampler is started and has delivered a first sample before the region
+    begins; only samples stamped inside the region count (the first one after it when
+    the region is shorter than the interval)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, interval_ms: int = 25):
         self.gpu = gpu_index
+        self.interval_ms = interval_ms
         self.proc = None
+        self.samples = []
+        self.t0 = self.t1 = None
+
+    def _reader(self):
+        for line in self.proc.stdout:
+            if line.strip():
+                self.samples.append((time.monotonic(), line))
 
     def __enter__(self):
+        import threading
+
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.interval_ms)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._reader, daemon=True)
+            self.thread.start()
+            deadline = time.monotonic() + 10.0
+            while not self.samples and time.monotonic() < deadline and self.proc.poll() is None:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
+        self.t0 = time.monotonic()
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
+        self.t1 = time.monotonic()
         if self.proc:
+            # one more sample after the region, for regions shorter than the interval
+            deadline = time.monotonic() + 1.0
+            n = len(self.samples)
+            while len(self.samples) == n and time.monotonic() < deadline and self.proc.poll() is None:
+                time.sleep(0.005)
             self.proc.terminate()
             try:
-                out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+            self.thread.join(timeout=5)
+        inside = [l for t, l in self.samples if self.t0 <= t <= self.t1]
+        if not inside:
+            inside = [l for t, l in self.samples if t > self.t1][:1]
+        self.lines = inside
 
     def summary(self):
         sm, smax, reasons = [], None, set()
@@ -193,15 +220,34 @@ def run_ours(args, ws, rank, local):
         if dist:
             dist.barrier()
 
-    wl = blast_large(args.elements)
-    solver = FRSolver(wl.cfg)
-    U = wl.init(f"cuda:{local}")
+    # N > 1: one mesh of elements x (elements * N) rows, a row block of elements^2 per
+    # rank (weak scaling); every step exchanges one ghost element row with each
+    # neighbour over NCCL and evaluates the residual of the owned rows.
+    blk = None
+    if ws > 1:
+        from fr_sdg_b200.partition import exchange_ghost_rows, row_blocks
+
+        wl = blast_large(args.elements, ny=args.elements * ws)
+        blk = row_blocks(args.elements * ws, ws, periodic_y=False)[rank]
+        solver = FRSolver(wl.cfg)
+        solver.set_row_window(*blk.window())
+        U = wl.init(f"cuda:{local}", rows=(blk.row_base, blk.rows))
+        row_len = U.numel() // blk.rows
+    else:
+        wl = blast_large(args.elements)
+        solver = FRSolver(wl.cfg)
+        U = wl.init(f"cuda:{local}")
     F = torch.empty_like(U)
-    dofs = U.numel()
+    dofs = U.numel() if blk is None else blk.owned * row_len
     stream = torch.cuda.current_stream()
 
-    for _ in range(args.warmup):
+    def step():
+        if blk is not None:
+            exchange_ghost_rows(U, blk, row_len)
         solver.rhs_func(0.0, U, F)
+
+    for _ in range(args.warmup):
+        step()
     torch.cuda.synchronize()
 
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -213,6 +259,8 @@ def run_ours(args, ws, rank, local):
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
         for k in range(args.steps):
+            if blk is not None:
+                exchange_ghost_rows(U, blk, row_len)
             starts[k].record(stream)
             solver.rhs_func(0.0, U, F)
             ends[k].record(stream)
@@ -230,7 +278,7 @@ def run_ours(args, ws, rank, local):
 
     # ---- the same residual in FP32 (mixed-precision form), device-resident
     mixed = None
-    if not args.no_t_end:
+    if not args.no_t_end and ws == 1:
         U32 = U.float()
         F32 = torch.empty_like(U32)
         for _ in range(3):
@@ -252,7 +300,32 @@ def run_ours(args, ws, rank, local):
 
     # ---- end to end through the host-buffer entry point
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and blk is not None:
+        # host vectors through the public API: pinned U -> device, ghost exchange,
+        # residual, rhs -> pinned host
+        Uh = U.cpu().pin_memory()
+        Fh = torch.empty_like(Uh).pin_memory()
+        ke = max(1, min(args.steps, args.e2e_steps))
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(ke):
+            U.copy_(Uh, non_blocking=True)
+            step()
+            Fh.copy_(F, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ems = e0.elapsed_time(e1)
+        t = torch.tensor([ems], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+        e2e = {"value": ws * dofs * ke / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": Uh.numel() * 8,
+               "d2h_bytes_per_step": Fh.numel() * 8, "steps": ke,
+               "path": "pinned host U -> device, NCCL ghost-row exchange, frsdg_rhs, rhs -> pinned host (per rank)"}
+    elif not args.no_e2e:
         Uh = U.cpu().pin_memory()
         Fh = torch.empty_like(Uh).pin_memory()
         solver.rhs_func_host(0.0, Uh, Fh)  # allocates the staging buffers once
@@ -291,7 +364,7 @@ def run_ours(args, ws, rank, local):
     # (2) The curved isentropic vortex (64^2, p = 4, RK4, CFL 0.05) to t = 10 with its
     # L2 density error against the exact translated vortex.
     t_end = None
-    if not args.no_t_end:
+    if not args.no_t_end and ws == 1:
         from fr_sdg_b200.integrate import Integrator, cfl_time_step, l2_error, node_jacobian
         from fr_sdg_b200.workloads import exact_vortex, node_coords, pack2d, vortex_curved
 
@@ -394,10 +467,12 @@ def run_ours(args, ws, rank, local):
         "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD if args.elements == 1024 else f"{WORKLOAD} at {args.elements}^2",
-                   "elements": [args.elements, args.elements], "poly_deg": 5, "dofs_per_rank": dofs,
+                   "elements": [args.elements, args.elements * ws], "poly_deg": 5, "dofs_per_rank": dofs,
                    "state_bytes": dofs * 8,
                    "l2": f"inputs ({dofs * 8 / 1e9:.2f} GB) larger than L2 (126 MB); no flush",
-                   "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+                   "parallelism": (f"row-block domain decomposition x{ws} ({args.elements}x{args.elements * ws} "
+                                   "elements, one ghost element row exchanged with each neighbour per step over NCCL)")
+                   if ws > 1 else "single GPU"},
         "clocks": clk.summary(), "gpu_launches": args.steps, "roofline": roof, "e2e": e2e,
         "cpu_baseline": cpu, "bad_density_nodes": bad, "time_to_t_end": t_end, "mixed_precision": mixed,
     }
@@ -408,7 +483,7 @@ def run_ours(args, ws, rank, local):
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=10)

@@ -68,6 +68,7 @@ SIGNATURES = {
     "frsdg_rk_stage": (C.c_int, [_P, _D, _P, _P, _D, _P, _D, _D, _P, _P, _D, _P]),
     "frsdg_jac_blocks": (C.c_int, [_P, _D, _D, _P, _P, _P]),
     "frsdg_residual_f32": (C.c_int, [_P, _D, _P, _P, _P]),
+    "frsdg_set_row_window": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
     "frsdg_rk_stage_mixed": (C.c_int, [_P, _D, _P, _P, _D, _P, _D, _D, _P, _P, _P, _D, _P]),
     "frsdg_pc_setup": (C.c_int, [_P, _D, _D, _P, _P]),
     "frsdg_pc_apply": (C.c_int, [_P, _P, _P, _P]),

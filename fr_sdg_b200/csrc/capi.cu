@@ -153,7 +153,22 @@ struct frsdg_handle
     const double* jvp_U = nullptr;
     cudaStream_t last = nullptr;
     int          device = 0;
+    // row window (frsdg_set_row_window); win_rows == 0: the vectors are the whole mesh
+    int          win_rows = 0, win_base = 0, win_begin = 0, win_end = 0;
 };
+
+// Element count and vector length of the vectors the entry points see.
+static int64_t local_nelem(const frsdg_handle* h) { return h->win_rows ? int64_t(h->Nx) * h->win_rows : h->nelem; }
+static int64_t local_ntot(const frsdg_handle* h) { return local_nelem(h) * h->ndofs; }
+static void apply_window(const frsdg_handle* h, Fr2dArgs& a)
+{
+    if (!h->win_rows) return;
+    a.Ny = h->win_rows;
+    a.per_y = 0;  // periodic neighbours arrive as ghost rows
+    a.row_base = h->win_base;
+    a.row_begin = h->win_begin;
+    a.row_end = h->win_end;
+}
 
 static void free_handle(frsdg_handle* h)
 {
@@ -323,6 +338,9 @@ int frsdg_create(const frsdg_config* cfg, frsdg_handle** out)
         Fr2dArgs& a = h->a2;
         a.Nx = Nx;
         a.Ny = Ny;
+        a.row_base = 0;
+        a.row_begin = 0;
+        a.row_end = Ny;
         a.per_x = per_x;
         a.per_y = per_y;
         a.gas = gas;
@@ -520,6 +538,7 @@ int run_residual(frsdg_handle* h, int mode, double t, const double* U, const dou
         a.inv_h = 1.0 / hh;
         a.sigma = h->jvp_sigma;
         if (stage) a.st = *stage;
+        apply_window(h, a);
         if (mode == MODE_JVP) e = dispatch2d<cplx>(h->n, h->cfg.gas_law, h->cfg.riemann, h->geo, a, s);
         else e = dispatch2d<double>(h->n, h->cfg.gas_law, h->cfg.riemann, h->geo, a, s);
     }
@@ -610,6 +629,7 @@ static int run_residual_f32(frsdg_handle* h, int mode, double t, const float* U3
     a.out = out;
     a.out_f32 = out_f32 ? 1 : 0;
     if (stage) a.st = *stage;
+    apply_window(h, a);
     const cudaError_t e = dispatch2d<float>(h->n, h->cfg.gas_law, h->cfg.riemann, h->geo, a, s);
     if (e != cudaSuccess) return cuda_fail(e, "FP32 residual launch");
     return FRSDG_OK;
@@ -631,6 +651,38 @@ int frsdg_rk_stage_mixed(frsdg_handle* h, double t, const float* Us32, const dou
     return run_residual_f32(h, MODE_STAGE, t, Us32, out, false, &st, stream);
 }
 
+int frsdg_set_row_window(frsdg_handle* h, int row_base, int rows, int row_begin, int row_end)
+{
+    if (!h) return fail(FRSDG_ERR_ARG, "null argument");
+    if (h->cfg.dim != 2) return fail(FRSDG_ERR_UNSUPPORTED, "frsdg_set_row_window: 2D configurations only");
+    if (rows == 0)
+    {
+        h->win_rows = h->win_base = h->win_begin = h->win_end = 0;
+        return FRSDG_OK;
+    }
+    const int Ny = h->Ny;
+    if (rows < 0 || row_begin < 0 || row_end <= row_begin || row_end > rows || rows > Ny + 2)
+        return fail(FRSDG_ERR_ARG, "frsdg_set_row_window: need 0 <= row_begin < row_end <= rows <= Ny + 2");
+    const int g0 = row_base + row_begin, g1 = row_base + row_end;
+    if (g0 < 0 || g1 > Ny) return fail(FRSDG_ERR_ARG, "frsdg_set_row_window: computed rows outside the mesh");
+    const bool per_y = h->cfg.bc[FRSDG_TOP].kind == FRSDG_BC_PERIODIC;
+    // a side without a ghost row must be the physical edge; a ghost row across the
+    // physical edge exists only for periodic meshes
+    if (row_begin == 0 && (g0 != 0 || per_y))
+        return fail(FRSDG_ERR_ARG, "frsdg_set_row_window: the bottom side needs a ghost row");
+    if (row_end == rows && (g1 != Ny || per_y))
+        return fail(FRSDG_ERR_ARG, "frsdg_set_row_window: the top side needs a ghost row");
+    if (row_begin > 0 && g0 == 0 && !per_y)
+        return fail(FRSDG_ERR_ARG, "frsdg_set_row_window: ghost row below a non-periodic bottom edge");
+    if (row_end < rows && g1 == Ny && !per_y)
+        return fail(FRSDG_ERR_ARG, "frsdg_set_row_window: ghost row above a non-periodic top edge");
+    h->win_rows = rows;
+    h->win_base = row_base;
+    h->win_begin = row_begin;
+    h->win_end = row_end;
+    return FRSDG_OK;
+}
+
 int frsdg_jac_blocks(frsdg_handle* h, double t, double sigma, const double* U, double* blocks, void* stream)
 {
     if (!h || !U || !blocks) return fail(FRSDG_ERR_ARG, "null argument");
@@ -649,6 +701,7 @@ int frsdg_jac_blocks(frsdg_handle* h, double t, double sigma, const double* U, d
     a.h = h->cfg.csd_eps;
     a.inv_h = 1.0 / h->cfg.csd_eps;
     a.sigma = sigma;
+    apply_window(h, a);
     const cudaError_t e = dispatch2d<cplx>(h->n, h->cfg.gas_law, h->cfg.riemann, h->geo, a, s);
     if (e != cudaSuccess) return cuda_fail(e, "Jacobian-block launch");
     return FRSDG_OK;
@@ -674,7 +727,7 @@ int frsdg_pc_setup(frsdg_handle* h, double t, double sigma, const double* U, voi
         return cuda_fail(e, "cudaMemsetAsync");
     int rc = frsdg_jac_blocks(h, t, sigma, U, h->d_blocks, stream);
     if (rc) return rc;
-    if ((e = launch_block_inverse(h->d_blocks, h->d_inv, nd, h->nelem, h->d_singular, s)) != cudaSuccess)
+    if ((e = launch_block_inverse(h->d_blocks, h->d_inv, nd, local_nelem(h), h->d_singular, s)) != cudaSuccess)
         return cuda_fail(e, "block-inverse launch");
     unsigned long long nsing = 0;
     if ((e = cudaMemcpyAsync(&nsing, h->d_singular, sizeof(nsing), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
@@ -691,7 +744,7 @@ int frsdg_pc_apply(frsdg_handle* h, const double* r, double* z, void* stream)
     if (r == z) return fail(FRSDG_ERR_ARG, "frsdg_pc_apply: z must not alias r");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     h->last = s;
-    const cudaError_t e = launch_block_apply(h->d_inv, r, z, h->ndofs, h->nelem, s);
+    const cudaError_t e = launch_block_apply(h->d_inv, r, z, h->ndofs, local_nelem(h), s);
     if (e != cudaSuccess) return cuda_fail(e, "block-apply launch");
     return FRSDG_OK;
 }
@@ -705,9 +758,14 @@ int frsdg_post_step(frsdg_handle* h, double* U, void* stream)
     StabArgs a = h->st;
     a.dst = U;
     a.src = U;
+    if (h->win_rows)
+    {
+        a.Ny = h->win_rows;
+        a.per_y = 0;
+    }
     if (h->d_work)
     {
-        cudaError_t e = cudaMemcpyAsync(h->d_work, U, sizeof(double) * h->ntot, cudaMemcpyDeviceToDevice, s);
+        cudaError_t e = cudaMemcpyAsync(h->d_work, U, sizeof(double) * local_ntot(h), cudaMemcpyDeviceToDevice, s);
         if (e != cudaSuccess) return cuda_fail(e, "post-step copy");
         a.src = h->d_work;
     }
@@ -721,7 +779,7 @@ int frsdg_prim_to_cons(frsdg_handle* h, const double* prim, double* cons, void* 
     if (!h || !prim || !cons) return fail(FRSDG_ERR_ARG, "null argument");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     h->last = s;
-    cudaError_t e = launch_prim_to_cons(h->cfg.dim, h->n, h->nelem, prim, cons, s);
+    cudaError_t e = launch_prim_to_cons(h->cfg.dim, h->n, local_nelem(h), prim, cons, s);
     if (e != cudaSuccess) return cuda_fail(e, "prim_to_cons launch");
     return FRSDG_OK;
 }
@@ -735,7 +793,7 @@ int frsdg_rhs_host(frsdg_handle* h, double t, const double* U_host, double* rhs_
         cudaError_t e = cudaMalloc(&h->d_stage, sizeof(double) * 2 * h->ntot);
         if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(staging)");
     }
-    const size_t bytes = sizeof(double) * h->ntot;
+    const size_t bytes = sizeof(double) * local_ntot(h);
     cudaError_t  e = cudaMemcpyAsync(h->d_stage, U_host, bytes, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return cuda_fail(e, "H2D copy");
     int rc = run_residual(h, MODE_RHS, t, h->d_stage, nullptr, h->d_stage + h->ntot, stream);

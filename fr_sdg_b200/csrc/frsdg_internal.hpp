@@ -97,6 +97,9 @@ struct Fr2dArgs
     StageArgs st;
     int    nd;         // DOFs per element, 4 n^2
     int    out_f32;    // residual written as float (FP32 instantiation)
+    // row window (domain decomposition): the vectors hold Ny element rows starting at
+    // global row row_base; rows [row_begin, row_end) are computed, the others are ghosts
+    int    row_base, row_begin, row_end;
     int    exact_bc;   // complex scalars: differentiate the user-lambda boundary kinds too
     int    jac_cmode;  // MODE_JAC colouring: 0 checkerboard, 1 three-colour cycles (odd periodic)
     Ops    ops;

@@ -230,8 +230,8 @@ __device__ __forceinline__ bool face_prepare(const Fr2dArgs& a, bool exists, int
     {
         if (exists)
         {
-            const double2 nn = XF ? __ldg(reinterpret_cast<const double2*>(a.xnorm) + (int64_t(gJ) * (a.Nx + 1) + gI) * N + pos)
-                                  : __ldg(reinterpret_cast<const double2*>(a.ynorm) + (int64_t(gJ) * a.Nx + gI) * N + pos);
+            const double2 nn = XF ? __ldg(reinterpret_cast<const double2*>(a.xnorm) + (int64_t(gJ + a.row_base) * (a.Nx + 1) + gI) * N + pos)
+                                  : __ldg(reinterpret_cast<const double2*>(a.ynorm) + (int64_t(gJ + a.row_base) * a.Nx + gI) * N + pos);
             nx = nn.x;
             ny = nn.y;
         }
@@ -266,8 +266,8 @@ __device__ __forceinline__ bool face_prepare(const Fr2dArgs& a, bool exists, int
     sd[0].bc = bcM;
     sd[1].bc = bcP;
     // the ghost needs the global position of the face point and of its interior node
-    if (bcM) sd[0].e = -2 - (XF ? gJ * N + pos : gI * N + pos), sd[1].e = eP;
-    if (bcP) sd[1].e = -2 - (XF ? gJ * N + pos : gI * N + pos), sd[0].e = eM;
+    if (bcM) sd[0].e = -2 - (XF ? (gJ + a.row_base) * N + pos : gI * N + pos), sd[1].e = eP;
+    if (bcP) sd[1].e = -2 - (XF ? (gJ + a.row_base) * N + pos : gI * N + pos), sd[0].e = eM;
     return exists;
 }
 
@@ -310,7 +310,7 @@ __device__ __forceinline__ void face_jumps(const Fr2dArgs& a, int i0, int j0, bo
         double sc;
         if constexpr (GEO == GEO_CURVED)
         {
-            const double* mt = a.metrics + ((int64_t(j0 + e / TX) * a.Nx + (i0 + e % TX)) * NN + node) * 4 + (XF ? 0 : 2);
+            const double* mt = a.metrics + ((int64_t(j0 + e / TX + a.row_base) * a.Nx + (i0 + e % TX)) * NN + node) * 4 + (XF ? 0 : 2);
             const double2 m = __ldg(reinterpret_cast<const double2*>(mt));
             sc = sqrt(m.x * m.x + m.y * m.y);
         }
@@ -350,8 +350,8 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
 
     const int tid = threadIdx.x;
     const int Nx = a.Nx, Ny = a.Ny;
-    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
-    const int txe = min(TX, Nx - i0), tye = min(TY, Ny - j0);
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY + a.row_begin;
+    const int txe = min(TX, Nx - i0), tye = min(TY, a.row_end - j0);
     const GasParams g = a.gas;
 
     // ---- P1: nodes of the tile; the halo traces (x-left, x-right per tile row,
@@ -496,7 +496,7 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
                 S fv[N];
 #pragma unroll
                 for (int m = 0; m < N; ++m) fv[m] = Fc[m * N];
-                const double* mt = a.metrics + ((int64_t(j0 + e / TX) * Nx + (i0 + e % TX)) * NN + k) * 4 + 2;
+                const double* mt = a.metrics + ((int64_t(j0 + e / TX + a.row_base) * Nx + (i0 + e % TX)) * NN + k) * 4 + 2;
 #pragma unroll
                 for (int l = 0; l < N; ++l)
                 {
@@ -566,7 +566,7 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
 #pragma unroll
                 for (int m = 0; m < N; ++m) dG = dG + opD<R_t>(a.ops, k * N + m) * gr[m];
                 const double2 mx = __ldg(reinterpret_cast<const double2*>(
-                    a.metrics + ((int64_t(j0 + ty) * Nx + (i0 + tx)) * NN + l * N + k) * 4));
+                    a.metrics + ((int64_t(j0 + ty + a.row_base) * Nx + (i0 + tx)) * NN + l * N + k) * 4));
                 R = (R_t(mx.x) * dF + R_t(mx.y) * dG) + sC[(e * 4 + eq) * NN + l * N + k];
             }
             else
@@ -612,7 +612,7 @@ cudaError_t launch_fr2d_kernel(const Fr2dArgs& a, cudaStream_t st)
         if (e != cudaSuccess) return e;
         attr_done = true;
     }
-    dim3 grid((a.Nx + T::TX - 1) / T::TX, (a.Ny + T::TY - 1) / T::TY,
+    dim3 grid((a.Nx + T::TX - 1) / T::TX, (a.row_end - a.row_begin + T::TY - 1) / T::TY,
               a.mode == MODE_JAC ? (a.jac_cmode ? 9 : 2) * T::NN * 4 : 1);
     kern<<<grid, T::BT, T::bytes, st>>>(a);
     return cudaGetLastError();

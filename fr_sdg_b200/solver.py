@@ -36,6 +36,7 @@ class FRSolver:
         A.check(self._lib.frsdg_n_dofs(h, C.byref(n)), "frsdg_n_dofs")
         self.n_dofs = int(n.value)
         self.n_elems = cfg.n_elems[0] * (cfg.n_elems[1] if cfg.dim == 2 else 1)
+        self.n_dofs_global = self.n_dofs
 
     # -- lifetime ---------------------------------------------------------
     def close(self) -> None:
@@ -59,6 +60,17 @@ class FRSolver:
         for v in vs:
             if v.dtype != torch.float64 or not v.is_cuda or not v.is_contiguous() or v.numel() != self.n_dofs:
                 raise ValueError(f"expected a contiguous float64 CUDA vector of {self.n_dofs} entries")
+
+    def set_row_window(self, row_base: int, rows: int, row_begin: int, row_end: int) -> None:
+        """Work on a row block of the mesh (frsdg_set_row_window): vectors then hold
+        `rows` element rows from global row `row_base`, of which [row_begin, row_end)
+        are computed; rows = 0 restores the whole mesh."""
+        A.check(self._lib.frsdg_set_row_window(self._h, row_base, rows, row_begin, row_end), "frsdg_set_row_window")
+        cfg = self.cfg
+        nx = cfg.n_elems[0]
+        nd = self.n_dofs_global // (nx * cfg.n_elems[1])
+        self.n_elems = nx * (rows if rows else cfg.n_elems[1])
+        self.n_dofs = self.n_elems * nd
 
     # -- PETSc callbacks --------------------------------------------------
     def residual_kernel(self, t: float, U: torch.Tensor, R: torch.Tensor) -> None:

@@ -62,9 +62,11 @@ def make_config(dim: int = 2, p: int = 3, n_elems=(10, 10), box=(1.0, 1.0), rada
 
 
 # ---------------------------------------------------------------- geometry on the host
-def node_coords(cfg: A.frsdg_config, device="cpu") -> tuple[torch.Tensor, torch.Tensor]:
+def node_coords(cfg: A.frsdg_config, device="cpu", rows: tuple[int, int] | None = None) -> tuple[torch.Tensor, torch.Tensor]:
     """Physical (x, y) of every node, shaped (Ny, Nx, n, n) [j, i, l, k] (2D) or
-    (Nx, n) (1D).  Same analytic maps as the library's geometry policies."""
+    (Nx, n) (1D).  Same analytic maps as the library's geometry policies.
+    rows = (row_base, count): only `count` element rows from global row `row_base`
+    (rows outside [0, Ny) wrap around, as the ghost rows of a periodic partition)."""
     p = cfg.poly_deg
     x_ref = torch.tensor(reference_element(p)[0], dtype=torch.float64, device=device)
     if cfg.dim == 1:
@@ -74,7 +76,10 @@ def node_coords(cfg: A.frsdg_config, device="cpu") -> tuple[torch.Tensor, torch.
         return h * (e + 0.5 * (1.0 + x_ref[None, :])), None
     Nx, Ny = cfg.n_elems[0], cfg.n_elems[1]
     i = torch.arange(Nx, dtype=torch.float64, device=device)
-    j = torch.arange(Ny, dtype=torch.float64, device=device)
+    if rows is None:
+        j = torch.arange(Ny, dtype=torch.float64, device=device)
+    else:
+        j = torch.remainder(torch.arange(rows[0], rows[0] + rows[1], device=device), Ny).to(torch.float64)
     csi = (1.0 / Nx) * (i[None, :, None, None] + 0.5 * (1.0 + x_ref[None, None, None, :]))
     eta = (1.0 / Ny) * (j[:, None, None, None] + 0.5 * (1.0 + x_ref[None, None, :, None]))
     csi, eta = torch.broadcast_tensors(csi, eta)
@@ -235,18 +240,21 @@ def bump_channel(nx: int = 256, ny: int = 64, p: int = 3, mach: float = 0.5) -> 
                     notes={"p_out": p_out})
 
 
-def blast_large(n_elems: int = 1024, p: int = 5) -> Workload:
+def blast_large(n_elems: int = 1024, p: int = 5, ny: int | None = None) -> Workload:
     """2D radial blast on [0,1]^2, HLLC, Van der Waals (a=0.05, b=0.02, gamma=1.4),
-    SSP-RK3, 200 steps, WENO + shock sensor (CFL 0.01: p = 5)."""
+    SSP-RK3, 200 steps, WENO + shock sensor (CFL 0.01: p = 5).  ny > n_elems stacks
+    more rows of the same element size above it (box [0,1] x [0, ny/n_elems]): the
+    weak-scaling mesh of a row-block partition."""
     a, b, g = 0.05, 0.02, 1.4
-    cfg = make_config(dim=2, p=p, n_elems=(n_elems, n_elems), box=(1.0, 1.0), riemann="hllc",
+    ny = ny or n_elems
+    cfg = make_config(dim=2, p=p, n_elems=(n_elems, ny), box=(1.0, ny / n_elems), riemann="hllc",
                       gas="vdw", gamma=g, vdw=(a, b),
                       bcs={A.LEFT: A.BC_OUTFLOW, A.RIGHT: A.BC_OUTFLOW, A.TOP: A.BC_OUTFLOW,
                            A.BOTTOM: A.BC_OUTFLOW},
                       **SHOCK_STAB)
 
-    def init(device="cpu"):
-        x, y = node_coords(cfg, device)
+    def init(device="cpu", rows=None):
+        x, y = node_coords(cfg, device, rows)
         r = torch.sqrt((x - 0.5) ** 2 + (y - 0.5) ** 2)
         inside = r < 0.4
         rho = torch.where(inside, 1.0, 0.125).to(torch.float64)
@@ -254,7 +262,7 @@ def blast_large(n_elems: int = 1024, p: int = 5) -> Workload:
         zero = torch.zeros_like(rho)
         return pack2d(rho, zero, zero, rhoE("vdw", g, a, b, rho, zero, pr))
 
-    return Workload(f"blast_vdw_{n_elems}x{n_elems}_p{p}", cfg, "ssprk3", 0.01, None, 200, init)
+    return Workload(f"blast_vdw_{n_elems}x{ny}_p{p}", cfg, "ssprk3", 0.01, None, 200, init)
 
 
 def circular_explosion(n_elems: int, p: int, gas: str, gamma: float, vdw, r0: float, p_out: float,

@@ -173,6 +173,17 @@ int frsdg_jvp_prepare(frsdg_handle* h, double t, double sigma, const double* U);
  * ComplexStepJacobianStrategy::matmult (petsc_solver_impl.hpp:250-432). */
 int frsdg_jvp(frsdg_handle* h, const double* V, double* JV, void* stream);
 
+/* Row window for domain decomposition (2D; the reference's DMDA ghosted local view,
+ * physics_impl_2D.hpp:646-902, with the halo width one element row).  After this call
+ * every vector argument of the handle holds `rows` element rows of the mesh starting
+ * at global row `row_base` (DMDA layout within them); rows [row_begin, row_end) are
+ * computed and written, the others are ghost rows the caller fills from the
+ * neighbouring partitions before each call (one row below and above is read).  Sides
+ * without a ghost row must be the mesh's non-periodic edge; on a periodic mesh both
+ * sides need ghost rows (row_base may be -1).  Geometry is looked up at global rows.
+ * rows = 0 restores the whole-mesh view. */
+int frsdg_set_row_window(frsdg_handle* h, int row_base, int rows, int row_begin, int row_end);
+
 /* Mixed precision (2D; no reference counterpart -- the reference computes in FP64
  * only).  frsdg_residual_f32: R = residual_kernel evaluated in FP32 on an FP32 state.
  * frsdg_rk_stage_mixed: frsdg_rk_stage with the residual taken in FP32 from Us32 and the
