@@ -442,8 +442,21 @@ def run_ours(args, ws, rank, local):
             vortex_mixed = {"workload": vw.name, "seconds": mms2 / 1e3, "steps": mst.steps, "t_end": mst.t,
                             "scheme": "RK4 mixed (FP32 residual, FP64 stages), CUDA graphs of 64 steps",
                             "l2_density_error_vs_exact": float(merr[0]), "finite": vs.status() == 0}
+        # (5) The batched uneven workload: 512 seeded circular explosions (32^2..128^2,
+        # p = 2..6, ideal / Van der Waals, filter on, CFL 0.1) advanced together for 32
+        # SSP-RK3 steps each on a pool of streams, each instance replaying its own graph.
+        from fr_sdg_b200.batch import BatchedInstances, load_manifest
+
+        bi = BatchedInstances(load_manifest(), f"cuda:{local}")
+        br = bi.run(None, 0.1, n_steps=32, steps_per_graph=32)
+        batched = {"instances": br.instances, "dofs": br.dofs, "steps_per_instance": 32, "seconds": br.seconds,
+                   "stage_dof_residuals_per_s": br.stage_residuals / br.seconds,
+                   "finite_after_32_steps": br.finite,
+                   "scheme": "SSP-RK3 + spectral filter, 16 streams, one CUDA graph of 32 steps per instance"}
+        bi.close()
+        del bi
         t_end = {"vortex_curved_64x64_p4": vortex, "vortex_curved_64x64_p4_mixed": vortex_mixed,
-                 "blast_200_steps": blast, "sod1d_200_p3": sod}
+                 "blast_200_steps": blast, "sod1d_200_p3": sod, "batched_uneven_512": batched}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

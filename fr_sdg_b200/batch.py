@@ -1,0 +1,146 @@
+"""The batched uneven workload: many independent small FR problems run together.
+
+Instances are circular explosions (ProblemFactory2D<CircularExplosion>,
+factory.hpp:400-465) on [-1,1]^2 with Rusanov fluxes and outflow boundaries, drawn
+with numpy.random.default_rng(20261203) in the order {Nx, p, gas kind, gamma | (a, b),
+r0, p_out} per instance: Nx = Ny in {32, 48, 64, 96, 128}, p in {2..6}, ideal gas with
+gamma ~ U[1.3, 1.67] or Van der Waals with a ~ U[0.01, 0.1], b ~ U[0.01, 0.05],
+gamma = 1.4; density 1 / 0.125 and pressure 1 / p_out ~ U[0.05, 0.2] inside / outside
+r0 ~ U[0.3, 0.5].  The draws are committed as data/batched_uneven_512.json.
+
+Each instance has its own handle, state and time step (CFL on its own mesh).  They
+advance concurrently on a pool of CUDA streams, every instance replaying its own CUDA
+graph of 64 SSP-RK3 steps, so small meshes overlap on the GPU instead of leaving it
+idle one launch at a time.
+"""
+from __future__ import annotations
+
+import json
+from dataclasses import asdict, dataclass
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from .integrate import Integrator, cfl_time_step
+from .solver import FRSolver
+from .workloads import SHOCK_STAB, Workload, circular_explosion
+
+SEED = 20261203
+SIZES = (32, 48, 64, 96, 128)
+MANIFEST = Path(__file__).resolve().parent / "data" / "batched_uneven_512.json"
+
+
+@dataclass(frozen=True)
+class InstanceSpec:
+    n_elems: int
+    p: int
+    gas: str
+    gamma: float
+    vdw_a: float
+    vdw_b: float
+    r0: float
+    p_out: float
+
+
+def draw_instances(n: int = 512, seed: int = SEED) -> list[InstanceSpec]:
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        ne = int(rng.choice(SIZES))
+        p = int(rng.integers(2, 7))
+        vdw = bool(rng.integers(0, 2))
+        if vdw:
+            gamma, a, b = 1.4, float(rng.uniform(0.01, 0.1)), float(rng.uniform(0.01, 0.05))
+        else:
+            gamma, a, b = float(rng.uniform(1.3, 1.67)), 0.0, 0.0
+        r0 = float(rng.uniform(0.3, 0.5))
+        p_out = float(rng.uniform(0.05, 0.2))
+        out.append(InstanceSpec(ne, p, "vdw" if vdw else "ideal", gamma, a, b, r0, p_out))
+    return out
+
+
+def write_manifest(specs: list[InstanceSpec], path: Path = MANIFEST) -> None:
+    path.write_text(json.dumps({"seed": SEED, "instances": [asdict(s) for s in specs]}, indent=1) + "\n")
+
+
+def load_manifest(path: Path = MANIFEST) -> list[InstanceSpec]:
+    return [InstanceSpec(**d) for d in json.loads(path.read_text())["instances"]]
+
+
+def instance_workload(spec: InstanceSpec, stab: str = "filter") -> Workload:
+    """stab = "filter": the configured spectral filter; "weno": WENO + shock sensor with
+    the filter off (the settings of the reference's shock runs)."""
+    # the filter's cut-off mode is 2 (filter.hpp defaults); at p = 2 that is the top
+    # mode and the filter strength formula divides 0 by 0, so p = 2 instances cut at 1
+    wl = circular_explosion(spec.n_elems, spec.p, spec.gas, spec.gamma, (spec.vdw_a, spec.vdw_b), spec.r0,
+                            spec.p_out, filt_cut_off=min(2, spec.p - 1))
+    if stab == "weno":
+        c = wl.cfg
+        c.apply_filter = 0
+        c.apply_weno = 1
+        c.weno_gamma = SHOCK_STAB["weno_gamma"]
+        c.shock_threshold = SHOCK_STAB["threshold"]
+        c.shock_theta = SHOCK_STAB["theta"]
+    return wl
+
+
+@dataclass
+class BatchResult:
+    instances: int
+    dofs: int
+    stage_residuals: float    # sum over instances of DOFs x stages
+    seconds: float
+    finite: int               # instances whose health word stayed clear
+    steps: list
+
+
+class BatchedInstances:
+    """All instances of a batch, resident on one GPU."""
+
+    def __init__(self, specs: list[InstanceSpec], device, stab: str = "filter", streams: int = 16, init=None):
+        """init(cfg, device) -> state replaces the explosion initial states (tests)."""
+        self.device = torch.device(device)
+        self.items = []
+        for sp in specs:
+            wl = instance_workload(sp, stab)
+            s = FRSolver(wl.cfg)
+            U = wl.init(self.device) if init is None else init(wl.cfg, self.device)
+            self.items.append((wl, s, U, Integrator(s, "ssprk3")))
+        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(streams)]
+
+    @property
+    def dofs(self) -> int:
+        return sum(U.numel() for _, _, U, _ in self.items)
+
+    def close(self) -> None:
+        for _, s, _, _ in self.items:
+            s.close()
+        self.items = []
+
+    def run(self, t_end: float | None, cfl: float, graph: bool = True, n_steps: int | None = None,
+            steps_per_graph: int = 64) -> BatchResult:
+        """Advance every instance to t_end (or by n_steps steps) with its own CFL time
+        step; device-timed from the first launch to the last completion over all
+        streams."""
+        cur = torch.cuda.current_stream(self.device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        for _, s, _, _ in self.items:
+            s.status()
+        dts = [cfl_time_step(wl.cfg, U, cfl) for wl, _, U, _ in self.items]
+        e0.record(cur)
+        steps = []
+        for k, ((wl, s, U, it), dt) in enumerate(zip(self.items, dts)):
+            st = self.streams[k % len(self.streams)]
+            st.wait_stream(cur)
+            with torch.cuda.stream(st):
+                steps.append(it.run(U, dt, t_end=t_end, n_steps=n_steps, graph=graph,
+                                    steps_per_graph=steps_per_graph).steps)
+        for st in self.streams:
+            cur.wait_stream(st)
+        e1.record(cur)
+        torch.cuda.synchronize(self.device)
+        finite = sum(1 for _, s, _, _ in self.items if s.status() == 0)
+        stage = float(sum(3 * n * U.numel() for n, (_, _, U, _) in zip(steps, self.items)))
+        return BatchResult(len(self.items), self.dofs, stage, e0.elapsed_time(e1) / 1e3, finite, steps)
