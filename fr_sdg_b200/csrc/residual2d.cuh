@@ -458,70 +458,110 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
     }
     __syncthreads();
 
-    // ---- P2: face points and element columns.  Each face thread solves one x-face
-    // point and one y-face point (two independent Riemann problems in flight).
+    // ---- P2: face points and element columns.  When the block has threads to
+    // spare, each face thread solves one face point (x-faces, then y-faces, on
+    // separate warps) and the remaining warps differentiate the element columns;
+    // otherwise each face thread solves one x-face and one y-face point (two
+    // independent Riemann problems in flight) and the columns follow.
     constexpr int NXF = (TX + 1) * TY * N, NYF = TX * (TY + 1) * N, NCOL = TE * 4 * N;
     constexpr int NFP = NXF > NYF ? NXF : NYF;
     constexpr int PFP = round_up32(NFP), PCOL = round_up32(NCOL);
-    for (int t = tid; t < PFP + PCOL; t += BT)
-    {
-        if (t < PFP)
+    constexpr int PX = round_up32(NXF), PY = round_up32(NYF);
+#ifdef FRSDG_PAIRED
+    constexpr bool UNPAIR = false;
+#else
+    constexpr bool UNPAIR = PX + PY < BT;
+#endif
+    auto column = [&](int tt) {
+        // column (e, eq, k): eta-derivatives of G (and of F on curved meshes)
+        const int k = tt % N, r = tt / N, eq = r % 4, e = r / 4;
+        if ((e % TX) >= txe || (e / TX) >= tye) return;
+        const S* Gc = sG + (e * 4 + eq) * NN + k;
+        S gv[N];
+#pragma unroll
+        for (int m = 0; m < N; ++m) gv[m] = Gc[m * N];
+        if constexpr (GEO == GEO_CURVED)
         {
-            FaceSide<S> xs[2], ys[2];
-            const bool vx = face_prepare<S, N, GEO, true>(a, t < NXF, t, i0, j0, txe, tye, sRec, xs);
-            const bool vy = face_prepare<S, N, GEO, false>(a, t < NYF, t, i0, j0, txe, tye, sRec, ys);
-            if (!vx && !vy) continue;
-            if (xs[0].bc || xs[1].bc) face_ghost<GAS, S, N, true>(a, i0, j0, xs);
-            if (ys[0].bc || ys[1].bc) face_ghost<GAS, S, N, false>(a, i0, j0, ys);
-            S Fx[4], Fy[4];
-            riemann_rec<RIEM>(xs[0].R, xs[1].R, xs[0].nx, xs[0].ny, Fx);
-            riemann_rec<RIEM>(ys[0].R, ys[1].R, ys[0].nx, ys[0].ny, Fy);
-            face_jumps<S, N, GEO, true>(a, i0, j0, vx, xs, Fx, sF, sG, sDel);
-            face_jumps<S, N, GEO, false>(a, i0, j0, vy, ys, Fy, sF, sG, sDel);
+            const S* Fc = sF + (e * 4 + eq) * NN + k;
+            S fv[N];
+#pragma unroll
+            for (int m = 0; m < N; ++m) fv[m] = Fc[m * N];
+            const double* mt = a.metrics + ((int64_t(j0 + e / TX + a.row_base) * Nx + (i0 + e % TX)) * NN + k) * 4 + 2;
+#pragma unroll
+            for (int l = 0; l < N; ++l)
+            {
+                S dG = S(0.0), dF = S(0.0);
+#pragma unroll
+                for (int m = 0; m < N; ++m)
+                {
+                    dG = dG + opD<R_t>(a.ops, l * N + m) * gv[m];
+                    dF = dF + opD<R_t>(a.ops, l * N + m) * fv[m];
+                }
+                const double2 me = __ldg(reinterpret_cast<const double2*>(mt + l * N * 4));
+                sC[(e * 4 + eq) * NN + l * N + k] = R_t(me.x) * dF + R_t(me.y) * dG;
+            }
         }
         else
         {
-            // column (e, eq, k): eta-derivatives of G (and of F on curved meshes)
-            const int tt = t - PFP;
-            if (tt >= NCOL) continue;
-            const int k = tt % N, r = tt / N, eq = r % 4, e = r / 4;
-            if ((e % TX) >= txe || (e / TX) >= tye) continue;
-            const S* Gc = sG + (e * 4 + eq) * NN + k;
-            S gv[N];
 #pragma unroll
-            for (int m = 0; m < N; ++m) gv[m] = Gc[m * N];
-            if constexpr (GEO == GEO_CURVED)
+            for (int l = 0; l < N; ++l)
             {
-                const S* Fc = sF + (e * 4 + eq) * NN + k;
-                S fv[N];
+                S dG = S(0.0);
 #pragma unroll
-                for (int m = 0; m < N; ++m) fv[m] = Fc[m * N];
-                const double* mt = a.metrics + ((int64_t(j0 + e / TX + a.row_base) * Nx + (i0 + e % TX)) * NN + k) * 4 + 2;
-#pragma unroll
-                for (int l = 0; l < N; ++l)
+                for (int m = 0; m < N; ++m) dG = dG + opD<R_t>(a.ops, l * N + m) * gv[m];
+                sC[(e * 4 + eq) * NN + l * N + k] = R_t(a.eta_y) * dG;
+            }
+        }
+    };
+    if constexpr (UNPAIR)
+    {
+        if (tid < PX + PY)
+        {
+            const bool xf = tid < PX;
+            const int t = xf ? tid : tid - PX;
+            FaceSide<S> sd[2];
+            S Fs[4];
+            if (xf)
+            {
+                if (face_prepare<S, N, GEO, true>(a, t < NXF, t, i0, j0, txe, tye, sRec, sd))
                 {
-                    S dG = S(0.0), dF = S(0.0);
-#pragma unroll
-                    for (int m = 0; m < N; ++m)
-                    {
-                        dG = dG + opD<R_t>(a.ops, l * N + m) * gv[m];
-                        dF = dF + opD<R_t>(a.ops, l * N + m) * fv[m];
-                    }
-                    const double2 me = __ldg(reinterpret_cast<const double2*>(mt + l * N * 4));
-                    sC[(e * 4 + eq) * NN + l * N + k] = R_t(me.x) * dF + R_t(me.y) * dG;
+                    if (sd[0].bc || sd[1].bc) face_ghost<GAS, S, N, true>(a, i0, j0, sd);
+                    riemann_rec<RIEM>(sd[0].R, sd[1].R, sd[0].nx, sd[0].ny, Fs);
+                    face_jumps<S, N, GEO, true>(a, i0, j0, true, sd, Fs, sF, sG, sDel);
                 }
             }
-            else
+            else if (face_prepare<S, N, GEO, false>(a, t < NYF, t, i0, j0, txe, tye, sRec, sd))
             {
-#pragma unroll
-                for (int l = 0; l < N; ++l)
-                {
-                    S dG = S(0.0);
-#pragma unroll
-                    for (int m = 0; m < N; ++m) dG = dG + opD<R_t>(a.ops, l * N + m) * gv[m];
-                    sC[(e * 4 + eq) * NN + l * N + k] = R_t(a.eta_y) * dG;
-                }
+                if (sd[0].bc || sd[1].bc) face_ghost<GAS, S, N, false>(a, i0, j0, sd);
+                riemann_rec<RIEM>(sd[0].R, sd[1].R, sd[0].nx, sd[0].ny, Fs);
+                face_jumps<S, N, GEO, false>(a, i0, j0, true, sd, Fs, sF, sG, sDel);
             }
+        }
+        else
+        {
+            for (int c = tid - PX - PY; c < NCOL; c += BT - PX - PY) column(c);
+        }
+    }
+    else
+    {
+        for (int t = tid; t < PFP + PCOL; t += BT)
+        {
+            if (t < PFP)
+            {
+                FaceSide<S> xs[2], ys[2];
+                const bool vx = face_prepare<S, N, GEO, true>(a, t < NXF, t, i0, j0, txe, tye, sRec, xs);
+                const bool vy = face_prepare<S, N, GEO, false>(a, t < NYF, t, i0, j0, txe, tye, sRec, ys);
+                if (!vx && !vy) continue;
+                if (xs[0].bc || xs[1].bc) face_ghost<GAS, S, N, true>(a, i0, j0, xs);
+                if (ys[0].bc || ys[1].bc) face_ghost<GAS, S, N, false>(a, i0, j0, ys);
+                S Fx[4], Fy[4];
+                riemann_rec<RIEM>(xs[0].R, xs[1].R, xs[0].nx, xs[0].ny, Fx);
+                riemann_rec<RIEM>(ys[0].R, ys[1].R, ys[0].nx, ys[0].ny, Fy);
+                face_jumps<S, N, GEO, true>(a, i0, j0, vx, xs, Fx, sF, sG, sDel);
+                face_jumps<S, N, GEO, false>(a, i0, j0, vy, ys, Fy, sF, sG, sDel);
+            }
+            else if (t - PFP < NCOL)
+                column(t - PFP);
         }
     }
     __syncthreads();
