@@ -149,6 +149,9 @@ struct frsdg_handle
     double*      d_blocks = nullptr;  // preconditioner: element-diagonal Jacobian blocks (FP64)
     float*       d_inv = nullptr;     // and their inverses (FP32); both allocated by the first frsdg_pc_setup
     unsigned long long* d_singular = nullptr;
+    double*      d_blocks5 = nullptr; // block Gauss-Seidel: the five blocks of every element row (FP64)
+    float*       d_off = nullptr;     // and the four off-diagonal ones in FP32; allocated by frsdg_pc_setup_gs
+    int          pc_kind = 0;         // 0 none, 1 block Jacobi, 2 block Gauss-Seidel
     double       jvp_t = 0.0, jvp_sigma = 1.0;
     const double* jvp_U = nullptr;
     cudaStream_t last = nullptr;
@@ -183,6 +186,8 @@ static void free_handle(frsdg_handle* h)
     cudaFree(h->d_blocks);
     cudaFree(h->d_inv);
     cudaFree(h->d_singular);
+    cudaFree(h->d_blocks5);
+    cudaFree(h->d_off);
     delete h;
 }
 
@@ -727,24 +732,94 @@ int frsdg_pc_setup(frsdg_handle* h, double t, double sigma, const double* U, voi
         return cuda_fail(e, "cudaMemsetAsync");
     int rc = frsdg_jac_blocks(h, t, sigma, U, h->d_blocks, stream);
     if (rc) return rc;
-    if ((e = launch_block_inverse(h->d_blocks, h->d_inv, nd, local_nelem(h), h->d_singular, s)) != cudaSuccess)
+    if ((e = launch_block_inverse(h->d_blocks, int64_t(nd) * nd, h->d_inv, nd, local_nelem(h), h->d_singular, s)) !=
+        cudaSuccess)
         return cuda_fail(e, "block-inverse launch");
     unsigned long long nsing = 0;
     if ((e = cudaMemcpyAsync(&nsing, h->d_singular, sizeof(nsing), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
         return cuda_fail(e, "pivot flag read");
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "pc setup sync");
     if (nsing) return fail(FRSDG_ERR_ARG, "frsdg_pc_setup: singular element block (zero pivot)");
+    h->pc_kind = 1;
+    return FRSDG_OK;
+}
+
+int frsdg_jac_blocks5(frsdg_handle* h, double t, double sigma, const double* U, double* blocks5, void* stream)
+{
+    if (!h || !U || !blocks5) return fail(FRSDG_ERR_ARG, "null argument");
+    if (h->cfg.dim != 2) return fail(FRSDG_ERR_UNSUPPORTED, "frsdg_jac_blocks5: 2D configurations only");
+    if (h->win_rows) return fail(FRSDG_ERR_UNSUPPORTED, "frsdg_jac_blocks5: whole-mesh handles only (no row window)");
+    const bool per_x = h->cfg.bc[FRSDG_LEFT].kind == FRSDG_BC_PERIODIC;
+    const bool per_y = h->cfg.bc[FRSDG_TOP].kind == FRSDG_BC_PERIODIC;
+    if ((per_x && h->Nx % 5) || (per_y && h->Ny % 5))
+        return fail(FRSDG_ERR_UNSUPPORTED, "frsdg_jac_blocks5: periodic directions need a multiple of 5 elements");
+    if ((reinterpret_cast<uintptr_t>(U) | reinterpret_cast<uintptr_t>(blocks5)) & 15)
+        return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    h->last = s;
+    Fr2dArgs a = h->a2;
+    a.t = t;
+    a.mode = MODE_JAC;
+    a.jac_cmode = 2;
+    a.cond_sys = h->cfg.cond_sys;
+    a.U = U;
+    a.W = nullptr;
+    a.out = blocks5;
+    a.h = h->cfg.csd_eps;
+    a.inv_h = 1.0 / h->cfg.csd_eps;
+    a.sigma = sigma;
+    const cudaError_t e = dispatch2d<cplx>(h->n, h->cfg.gas_law, h->cfg.riemann, h->geo, a, s);
+    if (e != cudaSuccess) return cuda_fail(e, "Jacobian-block launch");
+    return FRSDG_OK;
+}
+
+int frsdg_pc_setup_gs(frsdg_handle* h, double t, double sigma, const double* U, void* stream)
+{
+    if (!h || !U) return fail(FRSDG_ERR_ARG, "null argument");
+    if (h->cfg.dim != 2) return fail(FRSDG_ERR_UNSUPPORTED, "frsdg_pc_setup_gs: 2D configurations only");
+    if (h->cfg.bc[FRSDG_LEFT].kind == FRSDG_BC_PERIODIC || h->cfg.bc[FRSDG_TOP].kind == FRSDG_BC_PERIODIC)
+        return fail(FRSDG_ERR_UNSUPPORTED, "frsdg_pc_setup_gs: non-periodic meshes only");
+    const int nd = h->ndofs;
+    if (nd > kMaxBlockDofs) return fail(FRSDG_ERR_UNSUPPORTED, "frsdg_pc_setup_gs: element blocks above 144 DOFs (p > 5)");
+    cudaError_t e;
+    const size_t nb = size_t(h->nelem) * nd * nd;
+    if (!h->d_blocks5)
+    {
+        if ((e = cudaMalloc(&h->d_blocks5, sizeof(double) * 5 * nb)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(blocks)");
+        if ((e = cudaMalloc(&h->d_off, sizeof(float) * 4 * nb)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(blocks)");
+    }
+    if (!h->d_inv && (e = cudaMalloc(&h->d_inv, sizeof(float) * nb)) != cudaSuccess)
+        return cuda_fail(e, "cudaMalloc(inverse blocks)");
+    if (!h->d_singular && (e = cudaMalloc(&h->d_singular, sizeof(unsigned long long))) != cudaSuccess)
+        return cuda_fail(e, "cudaMalloc(pivot flag)");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if ((e = cudaMemsetAsync(h->d_singular, 0, sizeof(unsigned long long), s)) != cudaSuccess)
+        return cuda_fail(e, "cudaMemsetAsync");
+    int rc = frsdg_jac_blocks5(h, t, sigma, U, h->d_blocks5, stream);
+    if (rc) return rc;
+    if ((e = launch_block_inverse(h->d_blocks5, 5 * int64_t(nd) * nd, h->d_inv, nd, h->nelem, h->d_singular, s)) !=
+        cudaSuccess)
+        return cuda_fail(e, "block-inverse launch");
+    if ((e = launch_offdiag_to_f32(h->d_blocks5, h->d_off, nd, h->nelem, s)) != cudaSuccess)
+        return cuda_fail(e, "off-diagonal packing launch");
+    unsigned long long nsing = 0;
+    if ((e = cudaMemcpyAsync(&nsing, h->d_singular, sizeof(nsing), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return cuda_fail(e, "pivot flag read");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "pc setup sync");
+    if (nsing) return fail(FRSDG_ERR_ARG, "frsdg_pc_setup_gs: singular element block (zero pivot)");
+    h->pc_kind = 2;
     return FRSDG_OK;
 }
 
 int frsdg_pc_apply(frsdg_handle* h, const double* r, double* z, void* stream)
 {
     if (!h || !r || !z) return fail(FRSDG_ERR_ARG, "null argument");
-    if (!h->d_inv) return fail(FRSDG_ERR_ARG, "frsdg_pc_apply called before frsdg_pc_setup");
+    if (!h->pc_kind) return fail(FRSDG_ERR_ARG, "frsdg_pc_apply called before frsdg_pc_setup");
     if (r == z) return fail(FRSDG_ERR_ARG, "frsdg_pc_apply: z must not alias r");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     h->last = s;
-    const cudaError_t e = launch_block_apply(h->d_inv, r, z, h->ndofs, local_nelem(h), s);
+    const cudaError_t e = h->pc_kind == 2 ? launch_block_gs(h->d_inv, h->d_off, r, z, h->ndofs, h->Nx, h->Ny, s)
+                                          : launch_block_apply(h->d_inv, r, z, h->ndofs, local_nelem(h), s);
     if (e != cudaSuccess) return cuda_fail(e, "block-apply launch");
     return FRSDG_OK;
 }

@@ -101,7 +101,8 @@ struct Fr2dArgs
     // global row row_base; rows [row_begin, row_end) are computed, the others are ghosts
     int    row_base, row_begin, row_end;
     int    exact_bc;   // complex scalars: differentiate the user-lambda boundary kinds too
-    int    jac_cmode;  // MODE_JAC colouring: 0 checkerboard, 1 three-colour cycles (odd periodic)
+    int    jac_cmode;  // MODE_JAC colouring: 0 checkerboard, 1 three-colour cycles (odd periodic),
+                       // 2 distance-2 colouring (i + 2 j) mod 5 for all five blocks of an element row
     Ops    ops;
 };
 
@@ -111,6 +112,7 @@ struct Fr2dArgs
 __host__ __device__ inline int elem_colour(int cmode, int Nx, int Ny, int per_x, int per_y, int gi, int gj)
 {
     if (cmode == 0) return (gi + gj) & 1;
+    if (cmode == 2) return (gi + 2 * gj) % 5;
     const int cx = (per_x && (Nx & 1) && gi == Nx - 1) ? 2 : (gi & 1);
     const int cy = (per_y && (Ny & 1) && gj == Ny - 1) ? 2 : (gj & 1);
     return cx + 3 * cy;

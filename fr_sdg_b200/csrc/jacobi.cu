@@ -22,8 +22,9 @@ constexpr int kInvThreads = 256;
 // In-place inverse of the column-major n x n block A (a_ij at A[j n + i]) by
 // Gauss-Jordan elimination with row pivoting; the row exchanges are undone as
 // column exchanges at the end.  A zero pivot counts one singular block.
-__global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(const double* __restrict__ blocks, float* __restrict__ inv,
-                                                                    int n, unsigned long long* singular)
+__global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(const double* __restrict__ blocks, int64_t stride,
+                                                                    float* __restrict__ inv, int n,
+                                                                    unsigned long long* singular)
 {
     extern __shared__ double sA[];  // n * n doubles, n doubles of column k, n ints of pivot rows
     double* fcol = sA + n * n;
@@ -33,7 +34,7 @@ __global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(const double
     __shared__ int s_red_i[kInvThreads / 32];
     const int64_t base = int64_t(blockIdx.x) * n * n;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int q = tid; q < n * n; q += kInvThreads) sA[q] = blocks[base + q];
+    for (int q = tid; q < n * n; q += kInvThreads) sA[q] = blocks[int64_t(blockIdx.x) * stride + q];
     __syncthreads();
     bool bad = false;
     for (int k = 0; k < n; ++k)
@@ -130,18 +131,99 @@ __global__ void block_apply_kernel(const float* __restrict__ inv, const double* 
     }
 }
 
+// Off-diagonal blocks (slots 1-4 of each element's five) to FP32, packed four per element.
+__global__ void offdiag_to_f32_kernel(const double* __restrict__ blocks5, float* __restrict__ off, int64_t nel, int nn)
+{
+    const int64_t total = nel * 4 * nn;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < total; q += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int64_t e = q / (4 * nn), r = q - e * 4 * nn;  // r: (slot - 1) * nn + entry
+        off[q] = static_cast<float>(blocks5[e * 5 * nn + nn + r]);
+    }
+}
+
+// One colour half-sweep of the red-black block Gauss-Seidel preconditioner, one CTA
+// per element (elements of the other colour return at once).  Neighbour slots:
+// 0 right, 1 top, 2 bottom, 3 left (the off-diagonal blocks of slots 1-4).
+//   phase 0 (red):   z_e = inv_e r_e
+//   phase 1 (black): z_e = inv_e (r_e - sum_s J_es z_s)
+//   phase 2 (red):   z_e = z_e - inv_e (sum_s J_es z_s)
+__global__ void block_gs_kernel(const float* __restrict__ inv, const float* __restrict__ off,
+                                const double* __restrict__ r, double* __restrict__ z, int n, int Nx, int Ny, int phase)
+{
+    extern __shared__ double sv[];  // n: the vector the inverse multiplies; 4 n: neighbour values
+    const int64_t e = blockIdx.x;
+    const int gi = int(e % Nx), gj = int(e / Nx);
+    const int colour = (gi + gj) & 1;
+    if (colour != (phase == 1 ? 1 : 0)) return;
+    double* t = sv;
+    double* nbv = sv + n;
+    const int nbi[4] = {gi + 1 < Nx ? int(e) + 1 : -1, gj + 1 < Ny ? int(e) + Nx : -1, gj > 0 ? int(e) - Nx : -1,
+                        gi > 0 ? int(e) - 1 : -1};
+    if (phase > 0)
+    {
+        for (int q = threadIdx.x; q < 4 * n; q += blockDim.x)
+        {
+            const int s = q / n, j = q - s * n;
+            nbv[q] = nbi[s] >= 0 ? z[int64_t(nbi[s]) * n + j] : 0.0;
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+    {
+        double acc = 0.0;
+        if (phase > 0)
+            for (int s = 0; s < 4; ++s)
+            {
+                if (nbi[s] < 0) continue;
+                const float* B = off + (e * 4 + s) * int64_t(n) * n;
+                for (int j = 0; j < n; ++j) acc = fma(static_cast<double>(__ldg(B + int64_t(j) * n + i)), nbv[s * n + j], acc);
+            }
+        t[i] = phase == 0 ? r[e * n + i] : phase == 1 ? r[e * n + i] - acc : acc;
+    }
+    __syncthreads();
+    const float* Bi = inv + e * int64_t(n) * n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+    {
+        double acc = 0.0;
+        for (int j = 0; j < n; ++j) acc = fma(static_cast<double>(__ldg(Bi + int64_t(j) * n + i)), t[j], acc);
+        z[e * n + i] = phase == 2 ? z[e * n + i] - acc : acc;
+    }
+}
+
 } // namespace
 
 size_t block_inverse_smem(int n) { return size_t(n) * (n + 1) * sizeof(double) + size_t(n) * sizeof(int); }
 
-cudaError_t launch_block_inverse(const double* blocks, float* inv, int n, int64_t n_blocks, unsigned long long* singular,
-                                 cudaStream_t s)
+cudaError_t launch_block_inverse(const double* blocks, int64_t stride, float* inv, int n, int64_t n_blocks,
+                                 unsigned long long* singular, cudaStream_t s)
 {
     const size_t smem = block_inverse_smem(n);
     cudaError_t e = cudaFuncSetAttribute(block_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
-    block_inverse_kernel<<<unsigned(n_blocks), kInvThreads, smem, s>>>(blocks, inv, n, singular);
+    block_inverse_kernel<<<unsigned(n_blocks), kInvThreads, smem, s>>>(blocks, stride, inv, n, singular);
     return cudaGetLastError();
+}
+
+cudaError_t launch_offdiag_to_f32(const double* blocks5, float* off, int n, int64_t nel, cudaStream_t s)
+{
+    offdiag_to_f32_kernel<<<1184, 256, 0, s>>>(blocks5, off, nel, n * n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_block_gs(const float* inv, const float* off, const double* r, double* z, int n, int Nx, int Ny,
+                            cudaStream_t s)
+{
+    const int threads = n <= 64 ? 64 : n <= 128 ? 128 : 160;
+    const size_t smem = size_t(5 * n) * sizeof(double);
+    const unsigned nel = unsigned(int64_t(Nx) * Ny);
+    for (int phase = 0; phase < 3; ++phase)
+    {
+        block_gs_kernel<<<nel, threads, smem, s>>>(inv, off, r, z, n, Nx, Ny, phase);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_block_apply(const float* inv, const double* r, double* z, int n, int64_t n_blocks, cudaStream_t s)

@@ -584,8 +584,13 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
         const int64_t gbase = (int64_t(j0 + ty) * Nx + (i0 + tx)) * ND + eq;
         // coloured Jacobian: this slice's column d of the blocks of colour-c elements
         const int jz = int(blockIdx.z), jc = jz / ND, jd = jz % ND;
-        const bool jac_store = a.mode == MODE_JAC &&
-                               elem_colour(a.jac_cmode, Nx, Ny, a.per_x, a.per_y, i0 + tx, j0 + ty) == jc;
+        const int jcol = a.mode == MODE_JAC ? elem_colour(a.jac_cmode, Nx, Ny, a.per_x, a.per_y, i0 + tx, j0 + ty) : 0;
+        const bool jac_store = a.mode == MODE_JAC && (a.jac_cmode == 2 || jcol == jc);
+        // distance-2 colouring: the one element of colour jc in this element's face
+        // neighbourhood sits in slot (jc - colour) mod 5: 0 self, 1 right, 2 top, 3 bottom, 4 left
+        const int64_t jblk = a.jac_cmode == 2
+                                 ? (int64_t(j0 + ty) * Nx + (i0 + tx)) * 5 + (jc - jcol + 5) % 5
+                                 : (int64_t(j0 + ty) * Nx + (i0 + tx));
         S gr[N];
         if constexpr (GEO == GEO_CURVED)
         {
@@ -626,7 +631,7 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
                 jv += s_im(R) * a.inv_h;
                 if (a.mode != MODE_JAC) out[gidx] = jv;
                 else if (jac_store)
-                    out[(int64_t(j0 + ty) * Nx + (i0 + tx)) * int64_t(ND * ND) + int64_t(jd) * ND + (l * N + k) * 4 + eq] = jv;
+                    out[jblk * int64_t(ND * ND) + int64_t(jd) * ND + (l * N + k) * 4 + eq] = jv;
             }
             else if (a.out_f32)
                 reinterpret_cast<float*>(a.out)[gidx] = static_cast<float>(s_re(R));
@@ -653,7 +658,7 @@ cudaError_t launch_fr2d_kernel(const Fr2dArgs& a, cudaStream_t st)
         attr_done = true;
     }
     dim3 grid((a.Nx + T::TX - 1) / T::TX, (a.row_end - a.row_begin + T::TY - 1) / T::TY,
-              a.mode == MODE_JAC ? (a.jac_cmode ? 9 : 2) * T::NN * 4 : 1);
+              a.mode == MODE_JAC ? (a.jac_cmode == 2 ? 5 : a.jac_cmode ? 9 : 2) * T::NN * 4 : 1);
     kern<<<grid, T::BT, T::bytes, st>>>(a);
     return cudaGetLastError();
 }

@@ -9,7 +9,9 @@ module is the PETSc-free equivalent on the GPU:
 
   * J v       frsdg_jvp_prepare / frsdg_jvp (complex-step JVP kernel);
   * P^-1 r    frsdg_pc_setup / frsdg_pc_apply (element block-Jacobi: the diagonal
-              blocks of J from one coloured complex-step launch, FP32 inverses);
+              blocks of J from one coloured complex-step launch, FP32 inverses), or
+              frsdg_pc_setup_gs (red-black block Gauss-Seidel over all five blocks of an
+              element row, from one distance-2 coloured launch);
   * GMRES(m)  right-preconditioned, classical Gram-Schmidt applied twice (the
               Arnoldi basis lives on the device; the small Hessenberg least-squares
               problem is solved on the host with Givens rotations, Saad, "Iterative
@@ -29,6 +31,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
+from ._abi import FrsdgError
 from .solver import FRSolver
 
 
@@ -115,11 +118,13 @@ class BackwardEulerNewtonKrylov:
 
     def __init__(self, solver: FRSolver, restart: int = 30, gmres_rtol: float = 1e-3, max_gmres: int = 200,
                  newton_rtol: float = 1e-8, newton_atol: float = 1e-12, max_newton: int = 8,
-                 precondition: bool = True):
+                 precondition: bool | str = True):
+        """precondition: True / "jacobi" (element block-Jacobi), "gs" (red-black block
+        Gauss-Seidel over the five blocks of each element row) or False."""
         self.s = solver
         self.restart, self.gmres_rtol, self.max_gmres = restart, gmres_rtol, max_gmres
         self.newton_rtol, self.newton_atol, self.max_newton = newton_rtol, newton_atol, max_newton
-        self.precondition = precondition
+        self.precondition = "jacobi" if precondition is True else precondition
         self.cond_sys = bool(solver.cfg.cond_sys)
 
     def _transient(self, X: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
@@ -149,7 +154,10 @@ class BackwardEulerNewtonKrylov:
             if fn <= max(self.newton_rtol * f0, self.newton_atol) or it == self.max_newton:
                 break
             s.pre_jv_eval(t1, U, sigma)
-            if self.precondition:
+            if self.precondition == "gs":
+                s.pc_setup_gs(t1, sigma, U)
+                precond = s.pc_apply
+            elif self.precondition:
                 s.pc_setup(t1, sigma, U)
                 precond = s.pc_apply
             else:
@@ -175,12 +183,13 @@ class SteadyStats:
 
 def march_to_steady(solver: FRSolver, U: torch.Tensor, dt0: float, drop: float = 1e-10, max_steps: int = 200,
                     dt_max: float = 1e6, newton: BackwardEulerNewtonKrylov | None = None,
-                    max_rejections: int = 20) -> SteadyStats:
+                    max_rejections: int = 20, precondition: bool | str = True) -> SteadyStats:
     """Pseudo-transient continuation to a steady state: backward-Euler steps with the
     switched-evolution-relaxation time step until ||R(U)|| / ||R(U_0)|| <= drop.  A step
-    that leaves a non-finite residual or a non-positive density (frsdg_status) is
-    rejected and retried with a quarter of the time step, as a TS adaptor would."""
-    nk = newton or BackwardEulerNewtonKrylov(solver, restart=60, max_gmres=400, max_newton=1)
+    that leaves a non-finite residual or a non-positive density (frsdg_status), or meets
+    a singular element block in the preconditioner, is rejected and retried with a
+    quarter of the time step, as a TS adaptor would."""
+    nk = newton or BackwardEulerNewtonKrylov(solver, restart=60, max_gmres=400, max_newton=1, precondition=precondition)
     R = torch.empty_like(U)
     solver.residual_kernel(0.0, U, R)
     r0 = float(torch.linalg.vector_norm(R))
@@ -190,12 +199,16 @@ def march_to_steady(solver: FRSolver, U: torch.Tensor, dt0: float, drop: float =
     dt, t = dt0, 0.0
     while stats.steps < max_steps:
         U_prev.copy_(U)
-        st = nk.step(U, t, dt)
-        stats.newton_iterations += st.newton_iterations
-        stats.gmres_iterations += st.gmres_iterations
-        solver.residual_kernel(t + dt, U, R)
-        rk = float(torch.linalg.vector_norm(R))
-        if not math.isfinite(rk) or solver.status() != 0:
+        try:
+            st = nk.step(U, t, dt)
+        except FrsdgError:  # a singular element block at this state: reject the step
+            st = None
+        if st is not None:
+            stats.newton_iterations += st.newton_iterations
+            stats.gmres_iterations += st.gmres_iterations
+            solver.residual_kernel(t + dt, U, R)
+            rk = float(torch.linalg.vector_norm(R))
+        if st is None or not math.isfinite(rk) or solver.status() != 0:
             stats.rejected += 1
             if stats.rejected > max_rejections:
                 break

@@ -137,6 +137,20 @@ class FRSolver:
         self._check_vec(U)
         A.check(self._lib.frsdg_pc_setup(self._h, t, sigma, _ptr(U), _stream()), "frsdg_pc_setup")
 
+    def jac_blocks5(self, t: float, sigma: float, U: torch.Tensor, blocks5: torch.Tensor) -> None:
+        """All five blocks of every element row (distance-2 coloured complex step)."""
+        self._check_vec(U)
+        nd = self.n_dofs // self.n_elems
+        if blocks5.dtype != torch.float64 or not blocks5.is_cuda or not blocks5.is_contiguous() \
+                or blocks5.numel() != 5 * self.n_elems * nd * nd:
+            raise ValueError(f"expected a contiguous float64 CUDA tensor of {5 * self.n_elems * nd * nd} entries")
+        A.check(self._lib.frsdg_jac_blocks5(self._h, t, sigma, _ptr(U), _ptr(blocks5), _stream()), "frsdg_jac_blocks5")
+
+    def pc_setup_gs(self, t: float, sigma: float, U: torch.Tensor) -> None:
+        """Red-black block Gauss-Seidel preconditioner at (t, sigma, U)."""
+        self._check_vec(U)
+        A.check(self._lib.frsdg_pc_setup_gs(self._h, t, sigma, _ptr(U), _stream()), "frsdg_pc_setup_gs")
+
     def pc_apply(self, r: torch.Tensor, z: torch.Tensor) -> None:
         """z = inv(block diagonal) r."""
         self._check_vec(r, z)

@@ -214,6 +214,23 @@ int frsdg_jac_blocks(frsdg_handle* h, double t, double sigma, const double* U,
  * FRSDG_ERR_ARG on a zero pivot; p <= 5.  frsdg_pc_apply: z_e = inv(J_ee) r_e for
  * every element (z must not alias r). */
 int frsdg_pc_setup(frsdg_handle* h, double t, double sigma, const double* U, void* stream);
+
+/* All five blocks of every element row of the same Jacobian (the element and its four
+ * face neighbours) from one complex-step launch with the distance-2 colouring
+ * (i + 2 j) mod 5: blocks5: nelem * 5 * nd * nd doubles, block (e, s) column-major at
+ * ((e*5 + s)*nd + col)*nd + row, s = 0 self, 1 right, 2 top, 3 bottom, 4 left (zero where
+ * the neighbour does not exist).  2D, whole mesh; periodic directions need a multiple of
+ * 5 elements. */
+int frsdg_jac_blocks5(frsdg_handle* h, double t, double sigma, const double* U,
+                      double* blocks5, void* stream);
+
+/* Red-black block Gauss-Seidel preconditioner from those blocks (non-periodic 2D
+ * meshes, p <= 5): frsdg_pc_setup_gs computes them into handle-owned storage (first call
+ * allocates 5 nelem nd^2 doubles and 5 nelem nd^2 floats), inverts the diagonal blocks
+ * (FP64, partial pivoting, kept in FP32), keeps the couplings in FP32 and makes
+ * frsdg_pc_apply run one symmetric sweep: red z = D^-1 r; black z = D^-1 (r - J z_red);
+ * red z -= D^-1 J z_black.  Synchronises the stream; FRSDG_ERR_ARG on a zero pivot. */
+int frsdg_pc_setup_gs(frsdg_handle* h, double t, double sigma, const double* U, void* stream);
 int frsdg_pc_apply(frsdg_handle* h, const double* r, double* z, void* stream);
 
 /* One explicit Runge-Kutta stage fused into the residual pass:
