@@ -48,6 +48,24 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+# Nominal dense FP64 rate of a B200 (vector and tensor pipes alike); this pool's
+# measured peaks cover HBM and BF16 only.
+FP64_NOMINAL_TFLOPS = 37.0
+
+
+def flops_per_full_launch():
+    """Operations of one 1024^2 residual of the workload, counted on the reference
+    algorithm (oracle/count_flops.py -> profiles/fr2d_kernel_blast_flops.txt)."""
+    f = Path(__file__).resolve().parent / "profiles" / "fr2d_kernel_blast_flops.txt"
+    try:
+        for line in f.read_text().splitlines():
+            if line.startswith("flops_per_full_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def traffic_per_launch():
     """DRAM bytes per launch of the residual kernel from the committed ncu summary."""
     f = ROOT / "profiles" / "fr2d_kernel_blast_traffic.txt"
@@ -357,6 +375,16 @@ def run_ours(args, ws, rank, local):
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic_per_launch(), "peak_kind": peak_kind, "kernel": "fr2d_kernel<double,6,VdW,HLLC,affine>",
             "algorithmic_bytes_per_launch": alg_bytes, "mean_launch_ms": mean_launch_s * 1e3}
+    # the FP64 compute bound beside it: operations of the reference algorithm per launch
+    fl = flops_per_full_launch()
+    roof_fp64 = None
+    if fl is not None:
+        fl *= (args.elements / 1024) ** 2
+        tf = fl / mean_launch_s / 1e12
+        roof_fp64 = {"bound": "fp64", "achieved": tf, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                     "frac": tf / FP64_NOMINAL_TFLOPS, "peak_kind": "nominal (no measured FP64 peak on this pool)",
+                     "flops_per_launch": fl, "flop_per_algorithmic_byte": fl / alg_bytes,
+                     "count": "reference algorithm restated by the oracle, counting scalar (oracle/count_flops.py)"}
 
     # ---- time to t_end.  (1) The blast's own schedule (SSP-RK3, 200 steps, WENO with
     # the shock sensor), a throughput figure: the reference algorithm itself turns this
@@ -500,7 +528,7 @@ def run_ours(args, ws, rank, local):
                    "parallelism": (f"row-block domain decomposition x{ws} ({args.elements}x{args.elements * ws} "
                                    "elements, one ghost element row exchanged with each neighbour per step over NCCL)")
                    if ws > 1 else "single GPU"},
-        "clocks": clk.summary(), "gpu_launches": args.steps, "roofline": roof, "e2e": e2e,
+        "clocks": clk.summary(), "gpu_launches": args.steps, "roofline": roof, "roofline_fp64": roof_fp64, "e2e": e2e,
         "cpu_baseline": cpu, "bad_density_nodes": bad, "time_to_t_end": t_end, "mixed_precision": mixed,
     }
     print(json.dumps(line), flush=True)

@@ -48,6 +48,7 @@ def lib() -> C.CDLL:
             "oracle_filter_matrix": (C.c_int, [C.c_int, C.c_int, C.c_int, _D, _P]),
             "oracle_node_metrics": (C.c_int, [_P, _P]),
             "oracle_node_coords": (C.c_int, [_P, _P]),
+            "oracle_count_flops": (C.c_int, [_P, _D, _P, _P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -136,6 +137,14 @@ class Oracle:
         out = np.empty_like(prim)
         _chk(lib().oracle_prim_to_cons(self._h, _p(prim), _p(out)), "oracle_prim_to_cons")
         return out
+
+    def count_flops(self, t: float, U) -> dict:
+        """Arithmetic of one residual evaluation, counted by the counting scalar of
+        flop_count.cpp: additions, multiplications, divisions, square roots, exp/log/pow."""
+        U = self._vec(U)
+        c = np.zeros(5, dtype=np.uint64)
+        _chk(lib().oracle_count_flops(self._h, t, _p(U), c.ctypes.data), "oracle_count_flops")
+        return dict(zip(("add", "mul", "div", "sqrt", "other"), (int(v) for v in c)))
 
     def node_metrics(self) -> np.ndarray:
         out = np.empty(self.n_dofs // 4 * 5)

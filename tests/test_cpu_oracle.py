@@ -154,3 +154,22 @@ def test_oracle_complex_residual_real_part():
     Rc = o.residual_complex(0.0, U.astype(np.complex128))
     assert np.array_equal(Rc.real, o.residual(0.0, U))
     assert np.all(Rc.imag == 0.0)
+
+
+def test_flop_count_scales_with_elements():
+    """The oracle's counting scalar: a residual's operation count is deterministic and
+    grows as a M^2 + b M on M x M meshes (interior plus boundary faces)."""
+    from fr_sdg_b200.workloads import blast_large
+    from oracle.oracle import Oracle
+
+    counts = {}
+    for m in (4, 8, 16):
+        wl = blast_large(n_elems=m, p=2)
+        U = wl.init("cpu").numpy()
+        c1 = Oracle(wl.cfg).count_flops(0.0, U)
+        c2 = Oracle(wl.cfg).count_flops(0.0, U)
+        assert c1 == c2 and c1["add"] > 0 and c1["sqrt"] > 0 and c1["other"] == 0
+        counts[m] = sum(c1.values())
+    b = (counts[8] - 4 * counts[4]) / (8 - 16)
+    a = (counts[4] - 4 * b) / 16
+    assert abs(a * 256 + b * 16 - counts[16]) <= 1e-9 * counts[16]
