@@ -158,6 +158,10 @@ struct frsdg_handle
     int          device = 0;
     // row window (frsdg_set_row_window); win_rows == 0: the vectors are the whole mesh
     int          win_rows = 0, win_base = 0, win_begin = 0, win_end = 0;
+    // frsdg_rhs_host pipeline: upload / compute / download streams and their events
+    static constexpr int kHostChunks = 8;
+    cudaStream_t hst[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t  hev[2 * kHostChunks + 2] = {};
 };
 
 // Element count and vector length of the vectors the entry points see.
@@ -188,6 +192,10 @@ static void free_handle(frsdg_handle* h)
     cudaFree(h->d_singular);
     cudaFree(h->d_blocks5);
     cudaFree(h->d_off);
+    for (cudaStream_t& q : h->hst)
+        if (q) cudaStreamDestroy(q);
+    for (cudaEvent_t& ev : h->hev)
+        if (ev) cudaEventDestroy(ev);
     delete h;
 }
 
@@ -863,20 +871,87 @@ int frsdg_rhs_host(frsdg_handle* h, double t, const double* U_host, double* rhs_
 {
     if (!h || !U_host || !rhs_host) return fail(FRSDG_ERR_ARG, "null argument");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    h->last = s;
+    cudaError_t e;
     if (!h->d_stage)
     {
-        cudaError_t e = cudaMalloc(&h->d_stage, sizeof(double) * 2 * h->ntot);
+        e = cudaMalloc(&h->d_stage, sizeof(double) * 2 * h->ntot);
         if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(staging)");
     }
-    const size_t bytes = sizeof(double) * local_ntot(h);
-    cudaError_t  e = cudaMemcpyAsync(h->d_stage, U_host, bytes, cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) return cuda_fail(e, "H2D copy");
-    int rc = run_residual(h, MODE_RHS, t, h->d_stage, nullptr, h->d_stage + h->ntot, stream);
-    if (rc) return rc;
-    e = cudaMemcpyAsync(rhs_host, h->d_stage + h->ntot, bytes, cudaMemcpyDeviceToHost, s);
-    if (e != cudaSuccess) return cuda_fail(e, "D2H copy");
-    e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return cuda_fail(e, "stream sync");
+    double* dU = h->d_stage;
+    double* dR = h->d_stage + h->ntot;
+    constexpr int C = frsdg_handle::kHostChunks;
+    const bool chunked = h->cfg.dim == 2 && !h->win_rows && h->Ny >= 4 * C;
+    if (!chunked)
+    {
+        const size_t bytes = sizeof(double) * local_ntot(h);
+        if ((e = cudaMemcpyAsync(dU, U_host, bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+            return cuda_fail(e, "H2D copy");
+        int rc = run_residual(h, MODE_RHS, t, dU, nullptr, dR, stream);
+        if (rc) return rc;
+        if ((e = cudaMemcpyAsync(rhs_host, dR, bytes, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+            return cuda_fail(e, "D2H copy");
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "stream sync");
+        return FRSDG_OK;
+    }
+    // 2D whole mesh: C row chunks through three streams -- upload chunk c, compute it once
+    // its neighbour rows are there, download its rhs -- so that the host-to-device and
+    // device-to-host transfers overlap each other and the kernels.  The chunks are the
+    // kernel's row range on the whole arrays: the result is that of one launch.
+    if (!h->hst[0])
+    {
+        for (cudaStream_t& q : h->hst)
+            if ((e = cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking)) != cudaSuccess)
+                return cuda_fail(e, "cudaStreamCreate");
+        for (cudaEvent_t& ev : h->hev)
+            if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
+                return cuda_fail(e, "cudaEventCreate");
+    }
+    cudaEvent_t* up = h->hev;
+    cudaEvent_t* done = h->hev + C;
+    cudaEvent_t  start = h->hev[2 * C], finish = h->hev[2 * C + 1];
+    const int64_t row = int64_t(h->Nx) * h->ndofs;  // doubles per element row
+    auto r0 = [&](int c) { return c >= C ? h->Ny : int((int64_t(c) * h->Ny / C) & ~1); };
+    const bool per_y = h->a2.per_y;
+    if ((e = cudaEventRecord(start, s)) != cudaSuccess) return cuda_fail(e, "event record");
+    for (cudaStream_t q : h->hst)
+        if ((e = cudaStreamWaitEvent(q, start, 0)) != cudaSuccess) return cuda_fail(e, "stream wait");
+    for (int c = 0; c < C; ++c)
+    {
+        const size_t bytes = sizeof(double) * size_t(row) * size_t(r0(c + 1) - r0(c));
+        if ((e = cudaMemcpyAsync(dU + row * r0(c), U_host + row * r0(c), bytes, cudaMemcpyHostToDevice, h->hst[0])) !=
+            cudaSuccess)
+            return cuda_fail(e, "H2D copy");
+        if ((e = cudaEventRecord(up[c], h->hst[0])) != cudaSuccess) return cuda_fail(e, "event record");
+    }
+    // a periodic mesh's first chunk reads the last row: compute it last
+    for (int k = 0; k < C; ++k)
+    {
+        const int c = per_y ? (k + 1) % C : k;
+        const int need[3] = {c, c + 1 < C ? c + 1 : (per_y ? 0 : c), c > 0 ? c - 1 : (per_y ? C - 1 : c)};
+        for (int n : need)
+            if ((e = cudaStreamWaitEvent(h->hst[1], up[n], 0)) != cudaSuccess) return cuda_fail(e, "stream wait");
+        Fr2dArgs a = h->a2;
+        a.t = t;
+        a.mode = MODE_RHS;
+        a.cond_sys = 0;
+        a.U = dU;
+        a.W = nullptr;
+        a.out = dR;
+        a.row_begin = r0(c);
+        a.row_end = r0(c + 1);
+        if ((e = dispatch2d<double>(h->n, h->cfg.gas_law, h->cfg.riemann, h->geo, a, h->hst[1])) != cudaSuccess)
+            return cuda_fail(e, "residual launch");
+        if ((e = cudaEventRecord(done[c], h->hst[1])) != cudaSuccess) return cuda_fail(e, "event record");
+        if ((e = cudaStreamWaitEvent(h->hst[2], done[c], 0)) != cudaSuccess) return cuda_fail(e, "stream wait");
+        const size_t bytes = sizeof(double) * size_t(row) * size_t(r0(c + 1) - r0(c));
+        if ((e = cudaMemcpyAsync(rhs_host + row * r0(c), dR + row * r0(c), bytes, cudaMemcpyDeviceToHost, h->hst[2])) !=
+            cudaSuccess)
+            return cuda_fail(e, "D2H copy");
+    }
+    if ((e = cudaEventRecord(finish, h->hst[2])) != cudaSuccess) return cuda_fail(e, "event record");
+    if ((e = cudaStreamWaitEvent(s, finish, 0)) != cudaSuccess) return cuda_fail(e, "stream wait");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "stream sync");
     return FRSDG_OK;
 }
 
