@@ -393,112 +393,161 @@ def run_ours(args, ws, rank, local):
     # L2 density error against the exact translated vortex.
     t_end = None
     if not args.no_t_end and ws == 1:
-        from fr_sdg_b200.integrate import Integrator, cfl_time_step, l2_error, node_jacobian
-        from fr_sdg_b200.workloads import exact_vortex, node_coords, pack2d, vortex_curved
+        try:
+            from fr_sdg_b200.integrate import Integrator, cfl_time_step, l2_error, node_jacobian
+            from fr_sdg_b200.workloads import exact_vortex, node_coords, pack2d, vortex_curved
 
-        def timed(fn):
-            barrier()
+            def timed(fn):
+                barrier()
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                res = fn()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                barrier()
+                ms = e0.elapsed_time(e1)
+                if dist:
+                    tt = torch.tensor([ms], device=f"cuda:{local}")
+                    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+                    ms = float(tt.item())
+                return res, ms
+
+            # the first CUDA-graph capture of a process sets up the graph memory pool; do it
+            # once outside the timed runs
+            _warm = torch.zeros(8, device=f"cuda:{local}")
+            _g = torch.cuda.CUDAGraph()
+            _side = torch.cuda.Stream()
+            _side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(_side):
+                _g.capture_begin()
+                _warm.add_(1.0)
+                _g.capture_end()
+            torch.cuda.current_stream().wait_stream(_side)
+            _g.replay()
             torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            res = fn()
-            e1.record(stream)
-            torch.cuda.synchronize()
-            barrier()
-            ms = e0.elapsed_time(e1)
-            if dist:
-                tt = torch.tensor([ms], device=f"cuda:{local}")
-                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-                ms = float(tt.item())
-            return res, ms
+            del _g, _warm
+            U1 = wl.init(f"cuda:{local}")
+            dt = cfl_time_step(wl.cfg, U1, wl.cfl)
+            integ = Integrator(solver, "ssprk3")
+            integ.step(U1, 0.0, dt)  # warm (allocates the stage buffers)
+            U1.copy_(wl.init(f"cuda:{local}"))
+            solver.status()
+            st, ms = timed(lambda: integ.run(U1, dt, n_steps=wl.n_steps))
+            blast = {"seconds": ms / 1e3, "steps": st.steps, "dt": dt, "scheme": "SSP-RK3 + WENO/shock sensor",
+                     "stage_dof_residuals_per_s": ws * dofs * 3 * st.steps / (ms / 1e3),
+                     "finite": solver.status() == 0}
+            del U1, integ
+            vw = vortex_curved()
+            with FRSolver(vw.cfg) as vs:
+                V = vw.init(f"cuda:{local}")
+                vdt = cfl_time_step(vw.cfg, V, vw.cfl)
+                vint = Integrator(vs, "rk4")
+                vint.step(V, 0.0, vdt)
+                V.copy_(vw.init(f"cuda:{local}"))
+                vst, vms = timed(lambda: vint.run(V, vdt, t_end=vw.t_end, graph=True))
+                x, y = node_coords(vw.cfg, f"cuda:{local}")
+                err = l2_error(vw.cfg, V, pack2d(*exact_vortex(vst.t, x, y)), node_jacobian(vw.cfg, V.device))
+                vortex = {"workload": vw.name, "seconds": vms / 1e3, "steps": vst.steps, "t_end": vst.t, "dt": vdt,
+                          "scheme": "RK4, CUDA graphs of 64 steps", "l2_density_error_vs_exact": float(err[0]),
+                          "finite": vs.status() == 0}
+            # (3) The 1D Sod tube (200 elements, p = 3, SSP-RK3 + WENO, t = 0.2): launch-latency
+            # bound, so the full steps replay CUDA graphs; L1 density error against the exact
+            # Riemann solution (Toro, ch. 4).
+            from fr_sdg_b200 import refelem
+            from fr_sdg_b200.exact_riemann import sod_exact
+            from fr_sdg_b200.workloads import sod1d
+            sw = sod1d()
+            with FRSolver(sw.cfg) as ss:
+                S = sw.init(f"cuda:{local}")
+                sdt = cfl_time_step(sw.cfg, S, sw.cfl)
+                sint = Integrator(ss, "ssprk3")
+                sint.step(S, 0.0, sdt)
+                S.copy_(sw.init(f"cuda:{local}"))
+                sst, sms = timed(lambda: sint.run(S, sdt, t_end=sw.t_end, graph=True))
+                xs, _ = node_coords(sw.cfg, "cpu")
+                n1 = sw.cfg.poly_deg + 1
+                rho = S.view(-1, 3, n1)[:, 0].cpu().numpy()
+                w1 = np.array(refelem.reference_element(sw.cfg.poly_deg)[1]) * 0.5 / sw.cfg.n_elems[0]
+                l1 = float(np.sum(w1[None, :] * np.abs(rho - sod_exact(xs.numpy(), sst.t))))
+                sod = {"workload": sw.name, "seconds": sms / 1e3, "steps": sst.steps, "t_end": sst.t, "dt": sdt,
+                       "scheme": "SSP-RK3 + WENO/shock sensor, CUDA graphs of 64 steps",
+                       "l1_density_error_vs_exact": l1, "finite": ss.status() == 0}
+            # (4) The vortex again in mixed precision (FP32 residuals, FP64 stage sums)
+            with FRSolver(vw.cfg) as vs:
+                V = vw.init(f"cuda:{local}")
+                vint = Integrator(vs, "rk4", mixed=True)
+                vint.step(V, 0.0, vdt)
+                V.copy_(vw.init(f"cuda:{local}"))
+                mst, mms2 = timed(lambda: vint.run(V, vdt, t_end=vw.t_end, graph=True))
+                merr = l2_error(vw.cfg, V, pack2d(*exact_vortex(mst.t, x, y)), node_jacobian(vw.cfg, V.device))
+                vortex_mixed = {"workload": vw.name, "seconds": mms2 / 1e3, "steps": mst.steps, "t_end": mst.t,
+                                "scheme": "RK4 mixed (FP32 residual, FP64 stages), CUDA graphs of 64 steps",
+                                "l2_density_error_vs_exact": float(merr[0]), "finite": vs.status() == 0}
+            # (5) The batched uneven workload: 512 seeded circular explosions (32^2..128^2,
+            # p = 2..6, ideal / Van der Waals, filter on, CFL 0.1) advanced together for 32
+            # SSP-RK3 steps each on a pool of streams, each instance replaying its own graph.
+            from fr_sdg_b200.batch import BatchedInstances, load_manifest
 
-        # the first CUDA-graph capture of a process sets up the graph memory pool; do it
-        # once outside the timed runs
-        _warm = torch.zeros(8, device=f"cuda:{local}")
-        _g = torch.cuda.CUDAGraph()
-        _side = torch.cuda.Stream()
-        _side.wait_stream(torch.cuda.current_stream())
-        with torch.cuda.stream(_side):
-            _g.capture_begin()
-            _warm.add_(1.0)
-            _g.capture_end()
-        torch.cuda.current_stream().wait_stream(_side)
-        _g.replay()
-        torch.cuda.synchronize()
-        del _g, _warm
-        U1 = wl.init(f"cuda:{local}")
-        dt = cfl_time_step(wl.cfg, U1, wl.cfl)
-        integ = Integrator(solver, "ssprk3")
-        integ.step(U1, 0.0, dt)  # warm (allocates the stage buffers)
-        U1.copy_(wl.init(f"cuda:{local}"))
-        solver.status()
-        st, ms = timed(lambda: integ.run(U1, dt, n_steps=wl.n_steps))
-        blast = {"seconds": ms / 1e3, "steps": st.steps, "dt": dt, "scheme": "SSP-RK3 + WENO/shock sensor",
-                 "stage_dof_residuals_per_s": ws * dofs * 3 * st.steps / (ms / 1e3),
-                 "finite": solver.status() == 0}
-        del U1, integ
-        vw = vortex_curved()
-        with FRSolver(vw.cfg) as vs:
-            V = vw.init(f"cuda:{local}")
-            vdt = cfl_time_step(vw.cfg, V, vw.cfl)
-            vint = Integrator(vs, "rk4")
-            vint.step(V, 0.0, vdt)
-            V.copy_(vw.init(f"cuda:{local}"))
-            vst, vms = timed(lambda: vint.run(V, vdt, t_end=vw.t_end, graph=True))
-            x, y = node_coords(vw.cfg, f"cuda:{local}")
-            err = l2_error(vw.cfg, V, pack2d(*exact_vortex(vst.t, x, y)), node_jacobian(vw.cfg, V.device))
-            vortex = {"workload": vw.name, "seconds": vms / 1e3, "steps": vst.steps, "t_end": vst.t, "dt": vdt,
-                      "scheme": "RK4, CUDA graphs of 64 steps", "l2_density_error_vs_exact": float(err[0]),
-                      "finite": vs.status() == 0}
-        # (3) The 1D Sod tube (200 elements, p = 3, SSP-RK3 + WENO, t = 0.2): launch-latency
-        # bound, so the full steps replay CUDA graphs; L1 density error against the exact
-        # Riemann solution (Toro, ch. 4).
-        from fr_sdg_b200 import refelem
-        from fr_sdg_b200.exact_riemann import sod_exact
-        from fr_sdg_b200.workloads import sod1d
-        sw = sod1d()
-        with FRSolver(sw.cfg) as ss:
-            S = sw.init(f"cuda:{local}")
-            sdt = cfl_time_step(sw.cfg, S, sw.cfl)
-            sint = Integrator(ss, "ssprk3")
-            sint.step(S, 0.0, sdt)
-            S.copy_(sw.init(f"cuda:{local}"))
-            sst, sms = timed(lambda: sint.run(S, sdt, t_end=sw.t_end, graph=True))
-            xs, _ = node_coords(sw.cfg, "cpu")
-            n1 = sw.cfg.poly_deg + 1
-            rho = S.view(-1, 3, n1)[:, 0].cpu().numpy()
-            w1 = np.array(refelem.reference_element(sw.cfg.poly_deg)[1]) * 0.5 / sw.cfg.n_elems[0]
-            l1 = float(np.sum(w1[None, :] * np.abs(rho - sod_exact(xs.numpy(), sst.t))))
-            sod = {"workload": sw.name, "seconds": sms / 1e3, "steps": sst.steps, "t_end": sst.t, "dt": sdt,
-                   "scheme": "SSP-RK3 + WENO/shock sensor, CUDA graphs of 64 steps",
-                   "l1_density_error_vs_exact": l1, "finite": ss.status() == 0}
-        # (4) The vortex again in mixed precision (FP32 residuals, FP64 stage sums)
-        with FRSolver(vw.cfg) as vs:
-            V = vw.init(f"cuda:{local}")
-            vint = Integrator(vs, "rk4", mixed=True)
-            vint.step(V, 0.0, vdt)
-            V.copy_(vw.init(f"cuda:{local}"))
-            mst, mms2 = timed(lambda: vint.run(V, vdt, t_end=vw.t_end, graph=True))
-            merr = l2_error(vw.cfg, V, pack2d(*exact_vortex(mst.t, x, y)), node_jacobian(vw.cfg, V.device))
-            vortex_mixed = {"workload": vw.name, "seconds": mms2 / 1e3, "steps": mst.steps, "t_end": mst.t,
-                            "scheme": "RK4 mixed (FP32 residual, FP64 stages), CUDA graphs of 64 steps",
-                            "l2_density_error_vs_exact": float(merr[0]), "finite": vs.status() == 0}
-        # (5) The batched uneven workload: 512 seeded circular explosions (32^2..128^2,
-        # p = 2..6, ideal / Van der Waals, filter on, CFL 0.1) advanced together for 32
-        # SSP-RK3 steps each on a pool of streams, each instance replaying its own graph.
-        from fr_sdg_b200.batch import BatchedInstances, load_manifest
+            bi = BatchedInstances(load_manifest(), f"cuda:{local}")
+            br = bi.run(None, 0.1, n_steps=32, steps_per_graph=32)
+            batched = {"instances": br.instances, "dofs": br.dofs, "steps_per_instance": 32, "seconds": br.seconds,
+                       "stage_dof_residuals_per_s": br.stage_residuals / br.seconds,
+                       "finite_after_32_steps": br.finite,
+                       "scheme": "SSP-RK3 + spectral filter, 16 streams, one CUDA graph of 32 steps per instance"}
+            bi.close()
+            del bi
+            def implicit_figures():
+                # (6) The implicit path on the bump channel (256 x 64, p = 3, 1,048,576 DOF): the
+                # complex-step JVP, the two preconditioner set-ups and applies, and one backward-
+                # Euler step with Newton-GMRES and block Gauss-Seidel.
+                from fr_sdg_b200.implicit import BackwardEulerNewtonKrylov
+                from fr_sdg_b200.workloads import bump_channel
 
-        bi = BatchedInstances(load_manifest(), f"cuda:{local}")
-        br = bi.run(None, 0.1, n_steps=32, steps_per_graph=32)
-        batched = {"instances": br.instances, "dofs": br.dofs, "steps_per_instance": 32, "seconds": br.seconds,
-                   "stage_dof_residuals_per_s": br.stage_residuals / br.seconds,
-                   "finite_after_32_steps": br.finite,
-                   "scheme": "SSP-RK3 + spectral filter, 16 streams, one CUDA graph of 32 steps per instance"}
-        bi.close()
-        del bi
-        t_end = {"vortex_curved_64x64_p4": vortex, "vortex_curved_64x64_p4_mixed": vortex_mixed,
-                 "blast_200_steps": blast, "sod1d_200_p3": sod, "batched_uneven_512": batched}
+                bw = bump_channel()
+                with FRSolver(bw.cfg) as bs:
+                    B = bw.init(f"cuda:{local}")
+                    Vb = torch.rand_like(B)
+                    Jb = torch.empty_like(B)
+                    Zb = torch.empty_like(B)
+                    bs.pre_jv_eval(0.0, B, 10.0)
+                    bs.matmult(Vb, Jb)
+
+                    def rep(fn, n):
+                        _, ms_ = timed(lambda: [fn() for _ in range(n)])
+                        return ms_ / n
+
+                    jvp_ms = rep(lambda: bs.matmult(Vb, Jb), 20)
+                    bs.pc_setup(0.0, 10.0, B)
+                    pcj_setup_ms = rep(lambda: bs.pc_setup(0.0, 10.0, B), 3)
+                    pcj_apply_ms = rep(lambda: bs.pc_apply(Vb, Zb), 20)
+                    bs.pc_setup_gs(0.0, 10.0, B)
+                    pcg_setup_ms = rep(lambda: bs.pc_setup_gs(0.0, 10.0, B), 3)
+                    pcg_apply_ms = rep(lambda: bs.pc_apply(Vb, Zb), 20)
+                    nk = BackwardEulerNewtonKrylov(bs, restart=60, gmres_rtol=1e-6, max_gmres=600, newton_rtol=1e-8,
+                                                   precondition="gs")
+                    nst, nms = timed(lambda: nk.step(B, 0.0, 0.01))
+                    implicit = {"workload": bw.name, "dofs": B.numel(), "jvp_ms": jvp_ms,
+                                "jvp_dof_per_s": B.numel() / (jvp_ms / 1e3),
+                                "block_jacobi": {"setup_ms": pcj_setup_ms, "apply_ms": pcj_apply_ms},
+                                "block_gauss_seidel": {"setup_ms": pcg_setup_ms, "apply_ms": pcg_apply_ms},
+                                "backward_euler_step": {"dt": 0.01, "seconds": nms / 1e3,
+                                                        "newton_iterations": nst.newton_iterations,
+                                                        "gmres_iterations": nst.gmres_iterations,
+                                                        "f_drop": nst.f_norms[-1] / nst.f_norms[0]},
+                                "finite": bs.status() == 0}
+                return implicit
+
+            try:
+                implicit = implicit_figures()
+            except Exception as exc:  # an extra figure must not cost the headline line
+                implicit = {"error": f"{type(exc).__name__}: {exc}"}
+            t_end = {"vortex_curved_64x64_p4": vortex, "vortex_curved_64x64_p4_mixed": vortex_mixed,
+                     "blast_200_steps": blast, "sod1d_200_p3": sod, "batched_uneven_512": batched,
+                     "implicit_bump_256x64_p3": implicit}
+        except Exception as exc:  # the extra runs must not cost the headline line
+            t_end = {"error": f"{type(exc).__name__}: {exc}"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

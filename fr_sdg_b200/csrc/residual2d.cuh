@@ -648,14 +648,18 @@ cudaError_t launch_fr2d_kernel(const Fr2dArgs& a, cudaStream_t st)
 {
     using T = Tile2D<S, N, GEO>;
     auto kern = fr2d_kernel<S, N, GAS, RIEM, GEO>;
-    static bool attr_done = false;
-    if (!attr_done)
+    // kernel attributes are per device: set them once on each device that launches
+    static bool attr_done[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !attr_done[dev])
     {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(T::bytes));
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(T::bytes));
         if (e != cudaSuccess) return e;
         e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
-        attr_done = true;
+        if (dev >= 0 && dev < 64) attr_done[dev] = true;
     }
     dim3 grid((a.Nx + T::TX - 1) / T::TX, (a.row_end - a.row_begin + T::TY - 1) / T::TY,
               a.mode == MODE_JAC ? (a.jac_cmode == 2 ? 5 : a.jac_cmode ? 9 : 2) * T::NN * 4 : 1);
