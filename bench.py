@@ -40,6 +40,17 @@ def dist_env():
     return ws, rank, local
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (Linux /proc/cpuinfo), for the CPU-baseline record."""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -209,7 +220,7 @@ def run_reference(args, ws, rank):
         "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "parallelism": "host threads (OpenMP over element rows)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "cpu_model": cpu_model(),
                          "sample": info["sample"] + " per step; the reference binary needs PETSc/MPI/Eigen/Boost "
                                                     "and is not buildable here, so the oracle restatement runs"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -556,7 +567,7 @@ def run_ours(args, ws, rank, local):
         oracle.lib()
         threads = os.cpu_count() or 1
         r1, info1 = cpu_residual_rate(1, target_s=10.0, rows=16, max_reps=20)
-        cpu = {"value": r1, "unit": UNIT, "cores": 1, "kind": "port",
+        cpu = {"value": r1, "unit": UNIT, "cores": 1, "kind": "port", "cpu_model": cpu_model(),
                "sample": info1["sample"] + "; oracle restatement of the reference residual, 1 thread"}
         if args.cpu_all_cores:
             rN, infoN = cpu_residual_rate(threads, target_s=10.0, max_reps=20)
