@@ -68,7 +68,9 @@ class Integrator:
     (frsdg_rk_stage_mixed) and combines the stages in FP64; the FP64 state stays the
     solution.  The FP32 copy of U is refreshed at the end of every step."""
 
-    def __init__(self, solver: FRSolver, scheme: str = "ssprk3", mixed: bool = False):
+    def __init__(self, solver: FRSolver, scheme: str = "ssprk3", mixed: bool = False, before_stage=None):
+        """before_stage(V): called with every stage input and with U before the post-step
+        limiter -- a row-block partition refreshes its ghost rows there (FP64 stages)."""
         if scheme not in ("ssprk3", "rk4"):
             raise ValueError("scheme must be 'ssprk3' or 'rk4'")
         if mixed and (solver.cfg.dim != 2 or solver.cfg.cond_sys):
@@ -76,6 +78,9 @@ class Integrator:
         self.s = solver
         self.scheme = scheme
         self.mixed = mixed
+        self.before = before_stage
+        if mixed and before_stage is not None:
+            raise ValueError("before_stage: FP64 stages only")
         self._buf = None
         cfg = solver.cfg
         self.stabilise = bool(cfg.apply_filter or cfg.apply_weno)
@@ -105,6 +110,11 @@ class Integrator:
         if self.stabilise:
             s.apply_stabilization(U)
 
+    def _rk(self, t: float, Us: torch.Tensor, out: torch.Tensor, **kw) -> None:
+        if self.before is not None:
+            self.before(Us)
+        self.s.rk_stage(t, Us, out, **kw)
+
     def step(self, U: torch.Tensor, t: float, dt: float) -> None:
         """Advance U (in place) from t to t + dt, then apply the post-step limiter."""
         if self.mixed:
@@ -112,16 +122,18 @@ class Integrator:
         s = self.s
         b1, b2, b3 = self._buffers(U)[:3]
         if self.scheme == "ssprk3":
-            s.rk_stage(t, U, b1, gamma=dt, a=U, alpha=1.0)
-            s.rk_stage(t + dt, b1, b2, gamma=0.25 * dt, a=U, alpha=0.75, b=b1, beta=0.25)
-            s.rk_stage(t + 0.5 * dt, b2, U, gamma=2.0 * dt / 3.0, a=U, alpha=1.0 / 3.0, b=b2, beta=2.0 / 3.0)
+            self._rk(t, U, b1, gamma=dt, a=U, alpha=1.0)
+            self._rk(t + dt, b1, b2, gamma=0.25 * dt, a=U, alpha=0.75, b=b1, beta=0.25)
+            self._rk(t + 0.5 * dt, b2, U, gamma=2.0 * dt / 3.0, a=U, alpha=1.0 / 3.0, b=b2, beta=2.0 / 3.0)
         else:
             b3.copy_(U)
-            s.rk_stage(t, U, b1, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 6.0)
-            s.rk_stage(t + 0.5 * dt, b1, b2, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
-            s.rk_stage(t + 0.5 * dt, b2, b1, gamma=dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
-            s.rk_stage(t + dt, b1, U, gamma=dt / 6.0, a=b3, alpha=1.0)
+            self._rk(t, U, b1, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 6.0)
+            self._rk(t + 0.5 * dt, b1, b2, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
+            self._rk(t + 0.5 * dt, b2, b1, gamma=dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
+            self._rk(t + dt, b1, U, gamma=dt / 6.0, a=b3, alpha=1.0)
         if self.stabilise:
+            if self.before is not None:
+                self.before(U)
             s.apply_stabilization(U)
 
     def time_dependent(self) -> bool:
@@ -161,7 +173,7 @@ class Integrator:
         else:
             n_full = int(n_steps)
         t, k = t0, 0
-        if graph and n_full >= steps_per_graph and not self.time_dependent():
+        if graph and n_full >= steps_per_graph and not self.time_dependent() and self.before is None:
             g = self._capture(U, dt, steps_per_graph)
             for _ in range(n_full // steps_per_graph):
                 g.replay()

@@ -102,3 +102,20 @@ def exchange_ghost_rows(U_local, blk: RowBlock, row_len: int, group=None) -> Non
     if ops:
         for req in dist.batch_isend_irecv(ops):
             req.wait()
+
+
+def ghost_hook(blk: RowBlock, row_len: int, group=None):
+    """A stage hook for fr_sdg_b200.integrate.Integrator(before_stage=...): refreshes the
+    ghost rows of every stage input (and of the state before the post-step limiter)
+    from the neighbouring ranks."""
+    return lambda V: exchange_ghost_rows(V, blk, row_len, group)
+
+
+def global_max(x: float, device, group=None) -> float:
+    """Max over the ranks of a host scalar (the CFL time step's wave speed)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return float(t.item())
