@@ -79,6 +79,8 @@ SIGNATURES = {
     "frsdg_prim_to_cons": (C.c_int, [_P, _P, _P, _P]),
     "frsdg_rhs_host": (C.c_int, [_P, _D, _P, _P, _P]),
     "frsdg_status": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "frsdg_petsc_vec_record_bytes": (C.c_int, [C.c_int64, C.c_int32, C.POINTER(C.c_int64)]),
+    "frsdg_petsc_vec_pack": (C.c_int, [_P, C.c_int64, C.c_int32, _P, _P]),
     "frsdg_reference_element": (C.c_int, [C.c_int32, _D, _P, _P, _P, _P, _P]),
     "frsdg_filter_matrix": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _D, _P]),
 }

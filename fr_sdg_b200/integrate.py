@@ -161,10 +161,13 @@ class Integrator:
         return g
 
     def run(self, U: torch.Tensor, dt: float, t_end: float | None = None, n_steps: int | None = None,
-            t0: float = 0.0, graph: bool = False, steps_per_graph: int = 64) -> RunStats:
+            t0: float = 0.0, graph: bool = False, steps_per_graph: int = 64, monitor=None) -> RunStats:
         """March to t_end (last step clipped to land on it) or for n_steps steps.  With
         graph=True (and a residual that does not read t) the full steps replay a CUDA
-        graph of `steps_per_graph` steps; leftover and clipped steps run eagerly."""
+        graph of `steps_per_graph` steps; leftover and clipped steps run eagerly.
+        monitor(step, t, U, final) is called with the initial state (step 0) and after
+        every step (petsc_io.SolutionMonitor writes the PETSc solution file); a monitor
+        that writes intermediate steps keeps the run eager."""
         tol = 1e-14 * max(1.0, abs(t_end)) if t_end is not None else 0.0
         if t_end is not None:
             n_full = 0
@@ -172,8 +175,15 @@ class Integrator:
                 n_full += 1
         else:
             n_full = int(n_steps)
+        t_acc = t0
+        for _ in range(n_full):
+            t_acc += dt
+        n_total = n_full + (1 if t_end is not None and t_acc < t_end - tol else 0)
+        if monitor is not None:
+            monitor(0, t0, U, n_total == 0)
         t, k = t0, 0
-        if graph and n_full >= steps_per_graph and not self.time_dependent() and self.before is None:
+        if graph and n_full >= steps_per_graph and not self.time_dependent() and self.before is None and (
+                monitor is None or not monitor.every_step_matters):
             g = self._capture(U, dt, steps_per_graph)
             for _ in range(n_full // steps_per_graph):
                 g.replay()
@@ -181,15 +191,21 @@ class Integrator:
                     t += dt
                     k += 1
             del g
+            if monitor is not None and k == n_total:
+                monitor(k, t, U, True)
         while k < n_full:
             self.step(U, t, dt)
             t += dt
             k += 1
+            if monitor is not None:
+                monitor(k, t, U, k == n_total)
         if t_end is not None and t < t_end - tol:
             h = t_end - t
             self.step(U, t, h)
             t = t_end
             k += 1
+            if monitor is not None:
+                monitor(k, t, U, True)
         return RunStats(k, t, dt)
 
 

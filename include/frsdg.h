@@ -279,6 +279,21 @@ int frsdg_status(frsdg_handle* h, int64_t* bad_nodes);
  * Results equal frsdg_post_step's for the same configuration and input. */
 int frsdg_post_step_static(const frsdg_config* cfg, double* U, void* stream);
 
+/* PETSc binary Vec records, the file format of `-ts_monitor_solution binary:<file>`
+ * (options read by TSSetFromOptions, petsc_solver_impl.hpp:557; the record is
+ * written by PETSc's VecView) that the reference's tools read back
+ * (tools/plot.py:109-129, tools/check_iso_vortex.py:215-233).  One record = the
+ * class id 1211214 and the length n as big-endian integers of index_bytes bytes
+ * (4, or 8 for PETSc built with 64-bit indices), then n big-endian doubles.
+ *
+ * frsdg_petsc_vec_record_bytes: the record's size in bytes; FRSDG_ERR_ARG for
+ * index_bytes other than 4 or 8, or n > 2^31-1 with index_bytes = 4.
+ * frsdg_petsc_vec_pack: writes the record of the device vector x[0..n) into the
+ * device buffer out (record_bytes long) on `stream`, asynchronously; x and out
+ * 8-byte aligned.  A writer appends the bytes to the file as they are. */
+int frsdg_petsc_vec_record_bytes(int64_t n, int32_t index_bytes, int64_t* bytes);
+int frsdg_petsc_vec_pack(const double* x, int64_t n, int32_t index_bytes, void* out, void* stream);
+
 /* Host-only set-up operators, usable without a GPU.
  * Reference element: GLL (reference_element.hpp:50-147) and CachedElementData
  * (cached_computations.hpp:225-334).  Arrays: nodes[n], weights[n], D[n*n]
