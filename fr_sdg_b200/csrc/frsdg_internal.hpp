@@ -137,21 +137,30 @@ struct Fr1dArgs
 };
 
 // Tile of elements per CTA of the 2D kernel: TX along x (contiguous in memory)
-// by TY along y, about 200-400 nodes per tile.
+// by TY along y, about 100-400 nodes per tile, for the FP64 (words = 1), complex
+// (words = 2) and FP32 (f32) residuals.  face_tiles() selects the shapes sized by
+// face points (with the block size and register cap chosen in residual2d.cuh);
+// the others keep one thread per tile node.
 // FRSDG_TX / FRSDG_TY override the shape for tuning builds.
-__host__ __device__ constexpr int tile_x(int n)
+__host__ __device__ constexpr bool face_tiles(int n, int words, bool f32)
+{
+    return words == 1 && (f32 ? n == 6 : n >= 5);
+}
+__host__ __device__ constexpr int tile_x(int n, int words, bool f32)
 {
 #ifdef FRSDG_TX
     return FRSDG_TX;
 #else
+    if (face_tiles(n, words, f32)) return n == 5 ? 4 : 2;
     return n <= 2 ? 8 : n <= 3 ? 8 : n <= 4 ? 4 : n <= 6 ? 4 : 2;
 #endif
 }
-__host__ __device__ constexpr int tile_y(int n)
+__host__ __device__ constexpr int tile_y(int n, int words, bool f32)
 {
 #ifdef FRSDG_TY
     return FRSDG_TY;
 #else
+    if (face_tiles(n, words, f32)) return n == 5 ? 2 : n == 6 ? 4 : n <= 9 ? 2 : 1;
     return n <= 2 ? 8 : n <= 3 ? 4 : n <= 4 ? 4 : n <= 6 ? 2 : n <= 9 ? 2 : 1;
 #endif
 }

@@ -28,21 +28,37 @@ __host__ __device__ constexpr int round_up32(int v) { return (v + 31) / 32 * 32;
 
 // Block size and register cap of the 2D kernel (FRSDG_BT / FRSDG_MAXREG override
 // them for tuning builds).  A CTA's warps are spread over the SM's four
-// sub-partitions, each with a quarter of the register file, so the cap is chosen
-// for the number of co-resident CTAs wanted per SM.
-__host__ __device__ constexpr int block_threads(int n, int tile_nodes)
+// sub-partitions, each with a quarter of the register file.
+//   face tiles (FP64 at n >= 5, FP32 at n = 6): one thread per face point of the
+//     tile (x-face and y-face threads rounded to warps) plus one warp of element
+//     columns (two at n = 5), 80 registers, so that 4-6 CTAs share an SM;
+//   otherwise: one thread per tile node (128 to 512), the cap chosen for three
+//     co-resident CTAs (one for complex).
+// Measured on B200 (1024^2 blast rhs, FP64): p = 4 1.56 -> 1.41 ms, p = 5 1.77 ->
+// 1.57 ms, p = 6 4.17 -> 2.91 ms, p = 7 3.48 -> 3.36 ms, p = 8 4.21 -> 3.82 ms,
+// p = 9 6.79 -> 4.68 ms; at p = 2 and 3 one thread per node stays ahead (0.52 and
+// 0.86 ms against 0.62 and 0.95).  FP32: p = 5 1.00 -> 0.96 ms, but p = 4 0.75 ms
+// one thread per node against 0.85 ms.
+__host__ __device__ constexpr int face_threads(int n, int tx, int ty)
+{
+    return round_up32((tx + 1) * ty * n) + round_up32(tx * (ty + 1) * n);
+}
+__host__ __device__ constexpr int block_threads(int n, int words, bool f32, int tx, int ty)
 {
 #ifdef FRSDG_BT
     return FRSDG_BT;
 #else
+    if (face_tiles(n, words, f32)) return face_threads(n, tx, ty) + (n == 5 ? 64 : 32);
+    const int tile_nodes = tx * ty * n * n;
     return round_up32(tile_nodes > 128 ? (tile_nodes < 512 ? tile_nodes : 512) : 128);
 #endif
 }
-__host__ __device__ constexpr int reg_cap(int bt, int words)
+__host__ __device__ constexpr int reg_cap(int n, int words, bool f32, int bt)
 {
 #ifdef FRSDG_MAXREG
     return FRSDG_MAXREG;
 #else
+    if (face_tiles(n, words, f32)) return 80;
     // three co-resident CTAs (one for complex): per sub-partition ceil(ctas*warps/4) warps
     return (16384 / (32 * (((words == 2 ? 1 : 3) * (bt / 32) + 3) / 4))) / 8 * 8;
 #endif
@@ -50,13 +66,15 @@ __host__ __device__ constexpr int reg_cap(int bt, int words)
 
 template <class S, int N, int GEO> struct Tile2D
 {
-    static constexpr int TX = tile_x(N);
-    static constexpr int TY = tile_y(N);
+    static constexpr int W  = scalar_traits<S>::words;
+    static constexpr bool F32 = sizeof(S) == 4;
+    static constexpr int TX = tile_x(N, W, F32);
+    static constexpr int TY = tile_y(N, W, F32);
     static constexpr int NN = N * N;
     static constexpr int TE = TX * TY;
     static constexpr bool JVP = scalar_traits<S>::words == 2;
-    static constexpr int BT = block_threads(N, TE * NN);
-    static constexpr int MAXREG = reg_cap(BT, scalar_traits<S>::words) > 255 ? 255 : reg_cap(BT, scalar_traits<S>::words);
+    static constexpr int BT = block_threads(N, W, F32, TX, TY);
+    static constexpr int MAXREG = reg_cap(N, W, F32, BT) > 255 ? 255 : reg_cap(N, W, F32, BT);
     static constexpr int NB = 4 * N - 4;  // boundary nodes per element
     static constexpr int NREC_E = TE * NB;
     static constexpr int NHALO  = 2 * TY * N + 2 * TX * N;
@@ -275,7 +293,7 @@ __device__ __forceinline__ bool face_prepare(const Fr2dArgs& a, bool exists, int
 template <int GAS, class S, int N, bool XF>
 __device__ __forceinline__ void face_ghost(const Fr2dArgs& a, int i0, int j0, FaceSide<S> sd[2])
 {
-    constexpr int TX = tile_x(N), NN = N * N;
+    constexpr int TX = Tile2D<S, N, GEO_AFFINE>::TX, NN = N * N;
 #pragma unroll
     for (int side = 0; side < 2; ++side)
     {
@@ -298,7 +316,7 @@ template <class S, int N, int GEO, bool XF>
 __device__ __forceinline__ void face_jumps(const Fr2dArgs& a, int i0, int j0, bool valid, const FaceSide<S> sd[2],
                                            const S Fs[4], const S* sF, const S* sG, S* sDel)
 {
-    constexpr int TX = tile_x(N), NN = N * N;
+    constexpr int TX = Tile2D<S, N, GEO_AFFINE>::TX, NN = N * N;
     using R_t = typename scalar_traits<S>::real;
     if (!valid) return;
 #pragma unroll

@@ -12,6 +12,10 @@ module is the PETSc-free equivalent on the GPU:
               blocks of J from one coloured complex-step launch, FP32 inverses), or
               frsdg_pc_setup_gs (red-black block Gauss-Seidel over all five blocks of an
               element row, from one distance-2 coloured launch);
+  * coarse    optional second level (CoarseCorrection): the Galerkin operator
+              P^T J P on piecewise-constant aggregates of elements, probed with 20
+              JVPs (aggregates coloured (I + 2J) mod 5, four variables), factorised
+              densely; applied before the element-block sweep;
   * GMRES(m)  right-preconditioned, classical Gram-Schmidt applied twice (the
               Arnoldi basis lives on the device; the small Hessenberg least-squares
               problem is solved on the host with Givens rotations, Saad, "Iterative
@@ -31,6 +35,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
+from . import _abi as A
 from ._abi import FrsdgError
 from .solver import FRSolver
 
@@ -105,6 +110,101 @@ def gmres(matvec, precond, b: torch.Tensor, restart: int = 30, rtol: float = 1e-
     return x, GmresStats(total, rel)
 
 
+class CoarseCorrection:
+    """Second level of the preconditioner: z = P A_c^-1 P^T r with P the injection of
+    one constant state per aggregate of ax x ay elements (per variable) and
+    A_c = P^T J P the Galerkin coarse operator.
+
+    J couples an element to its face neighbours only, so J P couples an aggregate to
+    its four face-neighbour aggregates: colouring the aggregates by (I + 2J) mod 5
+    gives every closed five-aggregate neighbourhood distinct colours, and A_c follows
+    from 5 colours x 4 variables = 20 JVPs (the way the element blocks are probed by
+    frsdg_jac_blocks5).  A_c (4 * aggregates square, FP64) is LU-factorised once per
+    set-up; meshes of a few thousand aggregates keep it small."""
+
+    def __init__(self, cfg: A.frsdg_config, ax: int = 4, ay: int = 4):
+        if cfg.dim != 2:
+            raise ValueError("coarse correction: 2D meshes only")
+        for f in range(4):
+            if cfg.bc[f].kind == A.BC_PERIODIC:  # (I + 2J) mod 5 would need counts divisible by 5
+                raise ValueError("coarse correction: non-periodic meshes only")
+        self.nx, self.ny = cfg.n_elems[0], cfg.n_elems[1]
+        n = cfg.poly_deg + 1
+        self.nn = n * n
+        self.ax, self.ay = ax, ay
+        self.gx, self.gy = -(-self.nx // ax), -(-self.ny // ay)
+        self.nagg = self.gx * self.gy
+        self.nc = 4 * self.nagg
+        self._lu = None
+        self._dev = None
+
+    def _maps(self, device):
+        if self._dev != device:
+            i = torch.arange(self.nx, device=device)
+            j = torch.arange(self.ny, device=device)
+            I, J = (i // self.ax)[None, :], (j // self.ay)[:, None]
+            self.elem_agg = (J * self.gx + I).reshape(-1)            # aggregate of each element
+            gi = torch.arange(self.gx, device=device)[None, :]
+            gj = torch.arange(self.gy, device=device)[:, None]
+            self.colour = ((gi + 2 * gj) % 5).reshape(-1)             # colour of each aggregate
+            self._dev = device
+        return self.elem_agg
+
+    def restrict(self, r: torch.Tensor) -> torch.Tensor:
+        """P^T r: per aggregate and variable, the sum over its elements' nodes."""
+        ea = self._maps(r.device)
+        per_elem = r.view(-1, self.nn, 4).sum(1)
+        return torch.zeros(self.nagg, 4, dtype=r.dtype, device=r.device).index_add_(0, ea, per_elem)
+
+    def prolong(self, zc: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+        """out = P zc: every node of an aggregate takes the aggregate's state."""
+        ea = self._maps(out.device)
+        out.view(-1, self.nn, 4).copy_(zc.view(self.nagg, 4)[ea].unsqueeze(1).expand(-1, self.nn, 4))
+        return out
+
+    def neighbour_of_colour(self, c: int, device) -> torch.Tensor:
+        """For every aggregate, the aggregate of colour c in its closed face
+        neighbourhood (itself, right, top, bottom, left), or -1 when there is none."""
+        self._maps(device)
+        k = torch.arange(self.nagg, device=device)
+        I, J = k % self.gx, k // self.gx
+        d = (c - self.colour) % 5  # colour offsets: +1 right, -1 left, +2 top, -2 bottom
+        di = torch.where(d == 1, 1, torch.where(d == 4, -1, 0))
+        dj = torch.where(d == 2, 1, torch.where(d == 3, -1, 0))
+        I2, J2 = I + di, J + dj
+        ok = (I2 >= 0) & (I2 < self.gx) & (J2 >= 0) & (J2 < self.gy)
+        return torch.where(ok, J2 * self.gx + I2, torch.full_like(k, -1))
+
+    def assemble(self, matvec, template: torch.Tensor) -> torch.Tensor:
+        """A_c = P^T J P by coloured probing: 20 JVPs."""
+        dev = template.device
+        self._maps(dev)
+        A = torch.zeros(self.nagg, 4, self.nagg, 4, dtype=torch.float64, device=dev)
+        e = torch.empty_like(template)
+        w = torch.empty_like(template)
+        rows = torch.arange(self.nagg, device=dev)
+        for c in range(5):
+            src = self.neighbour_of_colour(c, dev)
+            has = src >= 0
+            sel = (self.colour == c).to(template.dtype)
+            for v in range(4):
+                zc = torch.zeros(self.nagg, 4, dtype=template.dtype, device=dev)
+                zc[:, v] = sel
+                matvec(self.prolong(zc, e), w)
+                rw = self.restrict(w)
+                A[rows[has], :, src[has], v] = rw[has]
+        return A.view(self.nc, self.nc)
+
+    def setup(self, matvec, template: torch.Tensor) -> None:
+        self._lu = torch.linalg.lu_factor(self.assemble(matvec, template))
+
+    def solve(self, r: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+        """out = P A_c^-1 P^T r."""
+        rc = self.restrict(r).reshape(self.nc, 1)
+        zc = torch.linalg.lu_solve(*self._lu, rc)
+        return self.prolong(zc, out)
+
+
 @dataclass
 class NewtonStats:
     newton_iterations: int
@@ -118,14 +218,34 @@ class BackwardEulerNewtonKrylov:
 
     def __init__(self, solver: FRSolver, restart: int = 30, gmres_rtol: float = 1e-3, max_gmres: int = 200,
                  newton_rtol: float = 1e-8, newton_atol: float = 1e-12, max_newton: int = 8,
-                 precondition: bool | str = True):
+                 precondition: bool | str = True, coarse: tuple[int, int] | None = None):
         """precondition: True / "jacobi" (element block-Jacobi), "gs" (red-black block
-        Gauss-Seidel over the five blocks of each element row) or False."""
+        Gauss-Seidel over the five blocks of each element row) or False.
+        coarse=(ax, ay): add the aggregate coarse level (CoarseCorrection) in front of
+        the element-block preconditioner: z = zc + M^-1 (r - J zc), zc = P A_c^-1 P^T r."""
         self.s = solver
         self.restart, self.gmres_rtol, self.max_gmres = restart, gmres_rtol, max_gmres
         self.newton_rtol, self.newton_atol, self.max_newton = newton_rtol, newton_atol, max_newton
         self.precondition = "jacobi" if precondition is True else precondition
         self.cond_sys = bool(solver.cfg.cond_sys)
+        if coarse and solver.n_dofs != solver.n_dofs_global:
+            raise ValueError("coarse correction: whole meshes only (no row window)")
+        self.coarse = CoarseCorrection(solver.cfg, *coarse) if coarse else None
+        self._w = None
+
+    def _two_level(self, smoother):
+        cc, s = self.coarse, self.s
+
+        def apply(r, z):
+            if self._w is None or self._w.shape != r.shape:
+                self._w = (torch.empty_like(r), torch.empty_like(r))
+            zc, w = self._w
+            cc.solve(r, zc)
+            s.matmult(zc, w)
+            torch.sub(r, w, out=w)
+            smoother(w, z)
+            z += zc
+        return apply
 
     def _transient(self, X: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
         if self.cond_sys:
@@ -163,6 +283,9 @@ class BackwardEulerNewtonKrylov:
             else:
                 def precond(r, z):
                     z.copy_(r)
+            if self.coarse is not None:
+                self.coarse.setup(s.matmult, U)
+                precond = self._two_level(precond)
             dx, g = gmres(s.matmult, precond, -F, restart=self.restart, rtol=self.gmres_rtol,
                           max_iter=self.max_gmres)
             U += dx

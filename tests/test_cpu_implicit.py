@@ -1,4 +1,6 @@
 """CPU: the host side of the implicit path (right-preconditioned GMRES)."""
+import numpy as np
+import pytest
 import torch
 
 from fr_sdg_b200.implicit import gmres
@@ -38,3 +40,75 @@ def test_gmres_residual_estimate_matches_true_residual():
     true = float(torch.linalg.vector_norm(A @ x - b) / torch.linalg.vector_norm(b))
     assert true <= 1e-4 * 1.01
     assert abs(true - st.residual) <= 1e-6
+
+
+def _face_coupled_operator(nx, ny, nd, seed):
+    """A random operator coupling each element to itself and its face neighbours,
+    the sparsity of the residual's Jacobian on a non-periodic mesh."""
+    rng = np.random.default_rng(seed)
+    n = nx * ny * nd
+    J = np.zeros((n, n))
+    for j in range(ny):
+        for i in range(nx):
+            e = j * nx + i
+            for di, dj in ((0, 0), (1, 0), (-1, 0), (0, 1), (0, -1)):
+                ii, jj = i + di, j + dj
+                if 0 <= ii < nx and 0 <= jj < ny:
+                    q = jj * nx + ii
+                    J[e * nd:(e + 1) * nd, q * nd:(q + 1) * nd] = rng.standard_normal((nd, nd))
+    return J
+
+
+@pytest.mark.parametrize("ax,ay", [(2, 2), (3, 2), (1, 1), (7, 5)])
+def test_coarse_operator_by_coloured_probing(ax, ay):
+    """CoarseCorrection.assemble (20 probes, aggregates coloured (I + 2J) mod 5) equals
+    P^T J P formed densely, on a 7 x 5 mesh with uneven aggregates."""
+    from fr_sdg_b200.implicit import CoarseCorrection
+    from fr_sdg_b200.workloads import make_config
+
+    cfg = make_config(dim=2, p=1, n_elems=(7, 5))
+    nx, ny, nn = 7, 5, 4
+    nd = 4 * nn
+    J = torch.from_numpy(_face_coupled_operator(nx, ny, nd, seed=ax * 10 + ay))
+    cc = CoarseCorrection(cfg, ax, ay)
+    # explicit P: column (K, v) = indicator of variable v on every node of aggregate K
+    P = torch.zeros(nx * ny * nd, cc.nc, dtype=torch.float64)
+    for k in range(cc.nc):
+        zc = torch.zeros(cc.nagg, 4, dtype=torch.float64)
+        zc.view(-1)[k] = 1.0
+        P[:, k] = cc.prolong(zc, torch.empty(nx * ny * nd, dtype=torch.float64))
+    ref = P.T @ J @ P
+    probes = []
+
+    def matvec(v, out):
+        probes.append(1)
+        out.copy_(J @ v)
+
+    got = cc.assemble(matvec, torch.zeros(nx * ny * nd, dtype=torch.float64))
+    assert len(probes) == 20
+    assert torch.allclose(got, ref, rtol=0, atol=1e-12 * float(ref.abs().max()))
+    # restriction is the transpose of the prolongation
+    r = torch.from_numpy(np.random.default_rng(3).standard_normal(nx * ny * nd))
+    assert torch.allclose(cc.restrict(r).reshape(-1), P.T @ r, atol=1e-12)
+
+
+def test_coarse_colouring_is_distance_two():
+    """Every aggregate's closed five-aggregate neighbourhood has five distinct colours,
+    and neighbour_of_colour finds the one of each colour."""
+    from fr_sdg_b200.implicit import CoarseCorrection
+    from fr_sdg_b200.workloads import make_config
+
+    cc = CoarseCorrection(make_config(dim=2, p=1, n_elems=(23, 11)), 2, 2)
+    cc._maps(torch.device("cpu"))
+    gx, gy = cc.gx, cc.gy
+    col = cc.colour.view(gy, gx)
+    for c in range(5):
+        nb = cc.neighbour_of_colour(c, torch.device("cpu"))
+        for k in range(cc.nagg):
+            I, Jj = k % gx, k // gx
+            hood = [(I + di, Jj + dj) for di, dj in ((0, 0), (1, 0), (-1, 0), (0, 1), (0, -1))
+                    if 0 <= I + di < gx and 0 <= Jj + dj < gy]
+            cols = [int(col[b, a]) for a, b in hood]
+            assert len(set(cols)) == len(cols)
+            match = [b * gx + a for a, b in hood if int(col[b, a]) == c]
+            assert int(nb[k]) == (match[0] if match else -1)
