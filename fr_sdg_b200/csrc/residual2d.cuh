@@ -377,9 +377,10 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
     static_assert(T::NHALO <= BT, "one halo node per thread");
     S hs[4];
     int hrec = -1;
-    if (tid < T::NHALO)
+    // the last NHALO threads carry the halo: the first threads may own two tile nodes
+    if (tid >= BT - T::NHALO)
     {
-        const int q = tid;
+        const int q = tid - (BT - T::NHALO);
         int ge_i, ge_j, node, r;
         bool ok;
         if (q < 2 * TY * N)

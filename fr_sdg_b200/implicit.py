@@ -237,7 +237,7 @@ class BackwardEulerNewtonKrylov:
         cc, s = self.coarse, self.s
 
         def apply(r, z):
-            if self._w is None or self._w.shape != r.shape:
+            if self._w is None or self._w[0].shape != r.shape:
                 self._w = (torch.empty_like(r), torch.empty_like(r))
             zc, w = self._w
             cc.solve(r, zc)
