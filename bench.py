@@ -505,8 +505,9 @@ def run_ours(args, ws, rank, local):
             br = bi.run(None, 0.1, n_steps=32, steps_per_graph=32)
             batched = {"instances": br.instances, "dofs": br.dofs, "steps_per_instance": 32, "seconds": br.seconds,
                        "stage_dof_residuals_per_s": br.stage_residuals / br.seconds,
-                       "finite_after_32_steps": br.finite,
-                       "scheme": "SSP-RK3 + spectral filter, 16 streams, one CUDA graph of 32 steps per instance"}
+                       "finite_after_32_steps": br.finite, "graph_capture_seconds": br.capture_seconds,
+                       "scheme": "SSP-RK3 + spectral filter, 16 streams, one CUDA graph of 32 steps per instance "
+                                 "(captured before the timed region, which holds the replays)"}
             bi.close()
             del bi
             def implicit_figures():

@@ -16,6 +16,7 @@ idle one launch at a time.
 from __future__ import annotations
 
 import json
+import time
 from dataclasses import asdict, dataclass
 from pathlib import Path
 
@@ -93,6 +94,7 @@ class BatchResult:
     seconds: float
     finite: int               # instances whose health word stayed clear
     steps: list
+    capture_seconds: float = 0.0  # host time spent capturing the graphs (before timing)
 
 
 class BatchedInstances:
@@ -122,25 +124,53 @@ class BatchedInstances:
             steps_per_graph: int = 64) -> BatchResult:
         """Advance every instance to t_end (or by n_steps steps) with its own CFL time
         step; device-timed from the first launch to the last completion over all
-        streams."""
+        streams.  With n_steps and graph=True every instance's graph of
+        steps_per_graph steps is captured before the timed region, which then holds
+        only graph replays (and the eager leftover steps)."""
         cur = torch.cuda.current_stream(self.device)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         for _, s, _, _ in self.items:
             s.status()
         dts = [cfl_time_step(wl.cfg, U, cfl) for wl, _, U, _ in self.items]
+        graphs, t_cap = None, 0.0
+        if graph and t_end is None and n_steps is not None and n_steps >= steps_per_graph:
+            c0 = time.perf_counter()
+            graphs = []
+            for k, ((_, _, U, it), dt) in enumerate(zip(self.items, dts)):
+                st = self.streams[k % len(self.streams)]
+                st.wait_stream(cur)
+                with torch.cuda.stream(st):
+                    graphs.append(it._capture(U, dt, steps_per_graph))
+            for st in self.streams:
+                cur.wait_stream(st)
+            torch.cuda.synchronize(self.device)
+            t_cap = time.perf_counter() - c0
         e0.record(cur)
         steps = []
         for k, ((wl, s, U, it), dt) in enumerate(zip(self.items, dts)):
             st = self.streams[k % len(self.streams)]
             st.wait_stream(cur)
             with torch.cuda.stream(st):
-                steps.append(it.run(U, dt, t_end=t_end, n_steps=n_steps, graph=graph,
-                                    steps_per_graph=steps_per_graph).steps)
+                if graphs is None:
+                    steps.append(it.run(U, dt, t_end=t_end, n_steps=n_steps, graph=graph,
+                                        steps_per_graph=steps_per_graph).steps)
+                    continue
+                reps = n_steps // steps_per_graph
+                for _ in range(reps):
+                    graphs[k].replay()
+                t = 0.0
+                for _ in range(reps * steps_per_graph):
+                    t += dt
+                for _ in range(n_steps - reps * steps_per_graph):
+                    it.step(U, t, dt)
+                    t += dt
+                steps.append(n_steps)
         for st in self.streams:
             cur.wait_stream(st)
         e1.record(cur)
         torch.cuda.synchronize(self.device)
+        del graphs
         finite = sum(1 for _, s, _, _ in self.items if s.status() == 0)
         stage = float(sum(3 * n * U.numel() for n, (_, _, U, _) in zip(steps, self.items)))
-        return BatchResult(len(self.items), self.dofs, stage, e0.elapsed_time(e1) / 1e3, finite, steps)
+        return BatchResult(len(self.items), self.dofs, stage, e0.elapsed_time(e1) / 1e3, finite, steps, t_cap)

@@ -11,6 +11,7 @@
 #include "jacobi.hpp"
 #include "stab.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -86,8 +87,6 @@ template <class S> cudaError_t dispatch1d(int n, int gas, int riem, const Fr1dAr
     }
 }
 
-bool is_native_bc(int k) { return k == FRSDG_BC_OUTFLOW || k == FRSDG_BC_WALL || k == FRSDG_BC_PERIODIC; }
-
 } // namespace
 
 namespace frsdg
@@ -159,7 +158,11 @@ struct frsdg_handle
     // row window (frsdg_set_row_window); win_rows == 0: the vectors are the whole mesh
     int          win_rows = 0, win_base = 0, win_begin = 0, win_end = 0;
     // frsdg_rhs_host pipeline: upload / compute / download streams and their events
-    static constexpr int kHostChunks = 8;
+#ifdef FRSDG_HOST_CHUNKS
+    static constexpr int kHostChunks = FRSDG_HOST_CHUNKS;  // tuning builds
+#else
+    static constexpr int kHostChunks = 32;  // at most; at least 4 element rows per chunk
+#endif
     cudaStream_t hst[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t  hev[2 * kHostChunks + 2] = {};
 };
@@ -880,8 +883,8 @@ int frsdg_rhs_host(frsdg_handle* h, double t, const double* U_host, double* rhs_
     }
     double* dU = h->d_stage;
     double* dR = h->d_stage + h->ntot;
-    constexpr int C = frsdg_handle::kHostChunks;
-    const bool chunked = h->cfg.dim == 2 && !h->win_rows && h->Ny >= 4 * C;
+    const int C = std::min(frsdg_handle::kHostChunks, h->Ny / 4);
+    const bool chunked = h->cfg.dim == 2 && !h->win_rows && C >= 2;
     if (!chunked)
     {
         const size_t bytes = sizeof(double) * local_ntot(h);
@@ -894,7 +897,8 @@ int frsdg_rhs_host(frsdg_handle* h, double t, const double* U_host, double* rhs_
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "stream sync");
         return FRSDG_OK;
     }
-    // 2D whole mesh: C row chunks through three streams -- upload chunk c, compute it once
+    // 2D whole mesh: C row chunks (up to 32: 5.1e9 -> 5.7e9 DOF/s against 8 on the 1024^2
+    // blast) through three streams -- upload chunk c, compute it once
     // its neighbour rows are there, download its rhs -- so that the host-to-device and
     // device-to-host transfers overlap each other and the kernels.  The chunks are the
     // kernel's row range on the whole arrays: the result is that of one launch.

@@ -144,7 +144,7 @@ struct Fr1dArgs
 // FRSDG_TX / FRSDG_TY override the shape for tuning builds.
 __host__ __device__ constexpr bool face_tiles(int n, int words, bool f32)
 {
-    return words == 1 && (f32 ? n == 6 : n >= 5);
+    return words == 1 && (f32 ? (n == 5 || n == 6) : n >= 5);
 }
 __host__ __device__ constexpr int tile_x(int n, int words, bool f32)
 {

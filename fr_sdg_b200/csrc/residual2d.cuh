@@ -29,7 +29,7 @@ __host__ __device__ constexpr int round_up32(int v) { return (v + 31) / 32 * 32;
 // Block size and register cap of the 2D kernel (FRSDG_BT / FRSDG_MAXREG override
 // them for tuning builds).  A CTA's warps are spread over the SM's four
 // sub-partitions, each with a quarter of the register file.
-//   face tiles (FP64 at n >= 5, FP32 at n = 6): one thread per face point of the
+//   face tiles (FP64 at n >= 5, FP32 at n = 5 and 6): one thread per face point of the
 //     tile (x-face and y-face threads rounded to warps) plus one warp of element
 //     columns (two at n = 5), 80 registers, so that 4-6 CTAs share an SM;
 //   otherwise: one thread per tile node (128 to 512), the cap chosen for three
@@ -37,8 +37,10 @@ __host__ __device__ constexpr int round_up32(int v) { return (v + 31) / 32 * 32;
 // Measured on B200 (1024^2 blast rhs, FP64): p = 4 1.56 -> 1.41 ms, p = 5 1.77 ->
 // 1.57 ms, p = 6 4.17 -> 2.91 ms, p = 7 3.48 -> 3.36 ms, p = 8 4.21 -> 3.82 ms,
 // p = 9 6.79 -> 4.68 ms; at p = 2 and 3 one thread per node stays ahead (0.52 and
-// 0.86 ms against 0.62 and 0.95).  FP32: p = 5 1.00 -> 0.96 ms, but p = 4 0.75 ms
-// one thread per node against 0.85 ms.
+// 0.86 ms against 0.62 and 0.95).  FP32: p = 5 1.00 -> 0.96 ms; at p = 4 one thread
+// per node is ahead on the 1024^2 mesh (0.75 against 0.85 ms) but behind on the 64^2
+// curved vortex of the mixed-precision runs (0.27 against 0.18 s to t = 10), which
+// fills fewer than two waves of CTAs, so FP32 takes face tiles at p = 4 and 5.
 __host__ __device__ constexpr int face_threads(int n, int tx, int ty)
 {
     return round_up32((tx + 1) * ty * n) + round_up32(tx * (ty + 1) * n);

@@ -151,10 +151,13 @@ class CoarseCorrection:
         return self.elem_agg
 
     def restrict(self, r: torch.Tensor) -> torch.Tensor:
-        """P^T r: per aggregate and variable, the sum over its elements' nodes."""
-        ea = self._maps(r.device)
-        per_elem = r.view(-1, self.nn, 4).sum(1)
-        return torch.zeros(self.nagg, 4, dtype=r.dtype, device=r.device).index_add_(0, ea, per_elem)
+        """P^T r: per aggregate and variable, the sum over its elements' nodes (plain
+        reductions in a fixed order, so repeated calls give identical bits)."""
+        per_elem = r.view(self.ny, self.nx, self.nn, 4).sum(2)
+        py, px = self.gy * self.ay - self.ny, self.gx * self.ax - self.nx
+        if px or py:
+            per_elem = torch.nn.functional.pad(per_elem, (0, 0, 0, px, 0, py))
+        return per_elem.view(self.gy, self.ay, self.gx, self.ax, 4).sum((1, 3)).reshape(self.nagg, 4)
 
     def prolong(self, zc: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
         """out = P zc: every node of an aggregate takes the aggregate's state."""
@@ -306,12 +309,15 @@ class SteadyStats:
 
 def march_to_steady(solver: FRSolver, U: torch.Tensor, dt0: float, drop: float = 1e-10, max_steps: int = 200,
                     dt_max: float = 1e6, newton: BackwardEulerNewtonKrylov | None = None,
-                    max_rejections: int = 20, precondition: bool | str = True) -> SteadyStats:
+                    max_rejections: int = 20, precondition: bool | str = True,
+                    max_growth: float | None = None, stall: float | None = None) -> SteadyStats:
     """Pseudo-transient continuation to a steady state: backward-Euler steps with the
     switched-evolution-relaxation time step until ||R(U)|| / ||R(U_0)|| <= drop.  A step
     that leaves a non-finite residual or a non-positive density (frsdg_status), or meets
     a singular element block in the preconditioner, is rejected and retried with a
-    quarter of the time step, as a TS adaptor would."""
+    quarter of the time step, as a TS adaptor would.  max_growth caps the ratio of
+    consecutive time steps; with stall, a step that leaves the residual above stall
+    times the previous one halves the time step instead of the SER update."""
     nk = newton or BackwardEulerNewtonKrylov(solver, restart=60, max_gmres=400, max_newton=1, precondition=precondition)
     R = torch.empty_like(U)
     solver.residual_kernel(0.0, U, R)
@@ -344,5 +350,10 @@ def march_to_steady(solver: FRSolver, U: torch.Tensor, dt0: float, drop: float =
         stats.history.append(stats.residual_drop)
         if stats.residual_drop <= drop:
             break
-        dt = min(dt0 / stats.residual_drop, dt_max)
+        prev = stats.history[-2]
+        if stall is not None and stats.residual_drop > stall * prev:
+            dt = 0.5 * dt
+            continue
+        dt_new = min(dt0 / stats.residual_drop, dt_max)
+        dt = dt_new if max_growth is None else min(dt_new, max_growth * dt)
     return stats
