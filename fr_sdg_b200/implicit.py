@@ -310,14 +310,16 @@ class SteadyStats:
 def march_to_steady(solver: FRSolver, U: torch.Tensor, dt0: float, drop: float = 1e-10, max_steps: int = 200,
                     dt_max: float = 1e6, newton: BackwardEulerNewtonKrylov | None = None,
                     max_rejections: int = 20, precondition: bool | str = True,
-                    max_growth: float | None = None, stall: float | None = None) -> SteadyStats:
+                    max_growth: float | None = None, stall: float | None = None,
+                    reject_growth: float | None = None) -> SteadyStats:
     """Pseudo-transient continuation to a steady state: backward-Euler steps with the
     switched-evolution-relaxation time step until ||R(U)|| / ||R(U_0)|| <= drop.  A step
     that leaves a non-finite residual or a non-positive density (frsdg_status), or meets
     a singular element block in the preconditioner, is rejected and retried with a
     quarter of the time step, as a TS adaptor would.  max_growth caps the ratio of
     consecutive time steps; with stall, a step that leaves the residual above stall
-    times the previous one halves the time step instead of the SER update."""
+    times the previous one halves the time step instead of the SER update; with
+    reject_growth, a step that multiplies the residual by more than that is rejected."""
     nk = newton or BackwardEulerNewtonKrylov(solver, restart=60, max_gmres=400, max_newton=1, precondition=precondition)
     R = torch.empty_like(U)
     solver.residual_kernel(0.0, U, R)
@@ -332,12 +334,15 @@ def march_to_steady(solver: FRSolver, U: torch.Tensor, dt0: float, drop: float =
             st = nk.step(U, t, dt)
         except FrsdgError:  # a singular element block at this state: reject the step
             st = None
+        rk = math.nan
         if st is not None:
             stats.newton_iterations += st.newton_iterations
             stats.gmres_iterations += st.gmres_iterations
             solver.residual_kernel(t + dt, U, R)
             rk = float(torch.linalg.vector_norm(R))
-        if st is None or not math.isfinite(rk) or solver.status() != 0:
+        bad = solver.status()  # read (and clear) the health word after every attempt
+        grew = reject_growth is not None and rk > reject_growth * stats.history[-1] * r0
+        if st is None or not math.isfinite(rk) or bad != 0 or grew:
             stats.rejected += 1
             if stats.rejected > max_rejections:
                 break
