@@ -838,6 +838,7 @@ int frsdg_pc_apply(frsdg_handle* h, const double* r, double* z, void* stream)
 int frsdg_post_step(frsdg_handle* h, double* U, void* stream)
 {
     if (!h || !U) return fail(FRSDG_ERR_ARG, "null argument");
+    if (reinterpret_cast<uintptr_t>(U) & 15) return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
     if (!h->cfg.apply_filter && !h->cfg.apply_weno) return FRSDG_OK;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     h->last = s;

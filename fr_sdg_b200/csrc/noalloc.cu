@@ -59,6 +59,7 @@ int scratch_address(double** out)
 extern "C" int frsdg_post_step_static(const frsdg_config* cfg, double* U, void* stream)
 {
     if (!cfg || !U) return report(FRSDG_ERR_ARG, "null argument");
+    if (reinterpret_cast<uintptr_t>(U) & 15) return report(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
     int rc = validate_config(*cfg);
     if (rc) return rc;
     const int n = cfg->poly_deg + 1;

@@ -84,52 +84,248 @@ __device__ void stab_line(const StabArgs& a, const double* prev, const double* c
     }
 }
 
-template <int N> __global__ void __launch_bounds__(kThreads) stab2d_kernel(const StabArgs a)
+// ---- 2D: tiles of elements staged in shared memory -------------------------
+// One CTA owns TX x TY elements.  It loads them, and for WENO the face neighbours
+// across the tile edges (left/right columns, bottom/top rows), into shared memory
+// with coalesced copies of whole elements; computes the smoothness indicator of
+// every line once (tile lines in both directions, halo lines in the direction that
+// crosses the tile edge), so each line's indicator serves the line itself and its
+// two neighbours; then limits each tile line and combines the x- and y-line results
+// per node, and stores the tile with coalesced writes.
+template <int N> struct StabTile
 {
-    constexpr int NN = N * N, ND = 4 * NN, LPE = 8 * N; // lines per element
-    constexpr int E = (kThreads / LPE) > 0 ? kThreads / LPE : 1;
-    __shared__ double sX[E * ND], sY[E * ND];
-    const int tid = threadIdx.x;
-    const int64_t nel = int64_t(a.Nx) * a.Ny;
-    const int64_t e0 = int64_t(blockIdx.x) * E;
-    const int le = tid / LPE, line = tid % LPE;
-    const int64_t ge = e0 + le;
-    const bool active = le < E && ge < nel;
-    if (active)
+    static constexpr int TX = N <= 6 ? 4 : 2, TY = TX;
+    static constexpr int TE = TX * TY, NN = N * N, ND = 4 * NN;
+    static constexpr int NSLOT = TE + 2 * TY + 2 * TX;          // tile, left, right, bottom, top
+    static constexpr int LX = 4 * N;                            // lines per element and direction
+    static constexpr int NBL = (2 * TE + 2 * TY + 2 * TX) * LX; // smoothness lines
+    static constexpr size_t bytes = sizeof(double) * (size_t(NSLOT) * ND + size_t(TE) * ND + NBL);
+};
+
+// WENOLimiter::compute_smoothness (filter.hpp:586-616) of one line
+template <int N> __device__ __forceinline__ double line_smoothness(const StabArgs& a, const double* v)
+{
+    double cur[N], nxt[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) cur[i] = v[i];
+    double beta = 0.0, factor = 4.0;
+#pragma unroll
+    for (int s = 1; s <= N - 1; ++s)
     {
-        const int gi = int(ge % a.Nx), gj = int(ge / a.Nx);
-        const bool xdir = line < 4 * N;
-        const int eq = (line % (4 * N)) / N, m = line % N;
-        auto elem = [&](int i, int j) -> const double* {
-            if (i < 0 || i >= a.Nx) { if (!a.per_x) return nullptr; i = (i + a.Nx) % a.Nx; }
-            if (j < 0 || j >= a.Ny) { if (!a.per_y) return nullptr; j = (j + a.Ny) % a.Ny; }
-            return a.src + (int64_t(j) * a.Nx + i) * ND;
-        };
-        const double* pC = elem(gi, gj);
-        const double* pP = xdir ? elem(gi - 1, gj) : elem(gi, gj - 1);
-        const double* pN = xdir ? elem(gi + 1, gj) : elem(gi, gj + 1);
-        double pv[N], cv[N], nv[N], o[N];
-        for (int t = 0; t < N; ++t)
+#pragma unroll
+        for (int r = 0; r < N; ++r)
         {
-            const int node = xdir ? (m * N + t) : (t * N + m);
-            cv[t] = pC[node * 4 + eq];
-            pv[t] = (a.apply_weno && pP) ? pP[node * 4 + eq] : 0.0;
-            nv[t] = (a.apply_weno && pN) ? pN[node * 4 + eq] : 0.0;
+            double acc = 0.0;
+#pragma unroll
+            for (int c = 0; c < N; ++c) acc += a.D[r * N + c] * cur[c];
+            nxt[r] = acc;
         }
-        stab_line<N>(a, pv, cv, nv, o);
-        double* dst = xdir ? sX : sY;
-        for (int t = 0; t < N; ++t)
+        double integ = 0.0;
+#pragma unroll
+        for (int i = 0; i < N; ++i)
         {
-            const int node = xdir ? (m * N + t) : (t * N + m);
-            dst[le * ND + node * 4 + eq] = o[t];
+            cur[i] = nxt[i];
+            integ += a.w[i] * cur[i] * cur[i];
         }
+        beta += factor * (0.5 * integ);
+        factor *= 4.0;
+    }
+    return beta;
+}
+
+// |x|^theta; theta = 1 (the shock runs' setting) is exactly |x|
+__device__ __forceinline__ double sensor_pow(double x, double theta) { return theta == 1.0 ? x : pow(x, theta); }
+
+// three CTAs per SM at n <= 6 (shared memory allows three there)
+template <int N> __global__ void __launch_bounds__(kThreads, N <= 6 ? 3 : 1) stab2d_tile_kernel(const StabArgs a)
+{
+    using T = StabTile<N>;
+    constexpr int TX = T::TX, TY = T::TY, TE = T::TE, ND = T::ND, LX = T::LX;
+    extern __shared__ __align__(16) unsigned char stab_smem[];
+    double* sU = reinterpret_cast<double*>(stab_smem);
+    double* sX = sU + T::NSLOT * ND;
+    double* sB = sX + TE * ND;
+    const int tid = threadIdx.x;
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+    const int txe = min(TX, a.Nx - i0), tye = min(TY, a.Ny - j0);
+    const bool weno = a.apply_weno && !a.apply_filter;
+    const int nslot = weno ? T::NSLOT : TE;
+
+    // global element of a slot, or -1 (outside the tile or a zero ghost across a
+    // non-periodic boundary)
+    auto slot_elem = [&](int sl) -> int64_t {
+        int i, j;
+        if (sl < TE)
+        {
+            const int tx = sl % TX, ty = sl / TX;
+            if (tx >= txe || ty >= tye) return -1;
+            i = i0 + tx;
+            j = j0 + ty;
+        }
+        else
+        {
+            const int h = sl - TE;
+            if (h < 2 * TY)
+            {
+                const int ty = h % TY;
+                if (ty >= tye) return -1;
+                i = h < TY ? i0 - 1 : i0 + txe;
+                j = j0 + ty;
+            }
+            else
+            {
+                const int tx = (h - 2 * TY) % TX;
+                if (tx >= txe) return -1;
+                i = i0 + tx;
+                j = h < 2 * TY + TX ? j0 - 1 : j0 + tye;
+            }
+            if (i < 0 || i >= a.Nx)
+            {
+                if (!a.per_x) return -1;
+                i = (i + a.Nx) % a.Nx;
+            }
+            if (j < 0 || j >= a.Ny)
+            {
+                if (!a.per_y) return -1;
+                j = (j + a.Ny) % a.Ny;
+            }
+        }
+        return int64_t(j) * a.Nx + i;
+    };
+
+    // stage the slots (whole elements, 16-byte copies)
+    for (int q = tid; q < nslot * (ND / 2); q += kThreads)
+    {
+        const int sl = q / (ND / 2), k = q % (ND / 2);
+        const int64_t ge = slot_elem(sl);
+        const double2 v = ge >= 0 ? __ldg(reinterpret_cast<const double2*>(a.src + ge * ND) + k) : make_double2(0.0, 0.0);
+        reinterpret_cast<double2*>(sU + sl * ND)[k] = v;
     }
     __syncthreads();
-    for (int q = tid; q < E * ND; q += kThreads)
+
+    // values of line li (eq = li % 4, m = li / 4) of a slot in direction dir
+    auto line_vals = [&](int sl, int dir, int li, double* v) {
+        const int eq = li % 4, m = li / 4;
+        const double* base = sU + sl * ND + eq;
+#pragma unroll
+        for (int t = 0; t < N; ++t) v[t] = base[(dir == 0 ? m * N + t : t * N + m) * 4];
+    };
+
+    if (weno)
     {
-        const int l2 = q / ND;
-        const int64_t g2 = e0 + l2;
-        if (g2 < nel) a.dst[g2 * ND + (q % ND)] = 0.5 * (sX[q] + sY[q]);
+        // smoothness of every line: tile x-lines, tile y-lines, then the halo slots
+        // (left, right: x-lines; bottom, top: y-lines), LX lines each
+        for (int b = tid; b < T::NBL; b += kThreads)
+        {
+            const int blk = b / LX, li = b % LX;
+            int sl, dir;
+            if (blk < TE) sl = blk, dir = 0;
+            else if (blk < 2 * TE) sl = blk - TE, dir = 1;
+            else sl = TE + (blk - 2 * TE), dir = (blk - 2 * TE) < 2 * TY ? 0 : 1;
+            double v[N];
+            line_vals(sl, dir, li, v);
+            sB[b] = line_smoothness<N>(a, v);
+        }
+        __syncthreads();
+    }
+
+    // limit the tile lines: x-lines into sX, then y-lines combined with them
+#pragma unroll 1
+    for (int dir = 0; dir < 2; ++dir)
+    {
+        for (int q = tid; q < TE * LX; q += kThreads)
+        {
+            const int e = q / LX, li = q % LX, tx = e % TX, ty = e / TX;
+            if (tx >= txe || ty >= tye) continue;
+            double cv[N], o[N];
+            line_vals(e, dir, li, cv);
+            if (weno)
+            {
+                int sp, sn, bp, bn;
+                if (dir == 0)
+                {
+                    sp = tx > 0 ? e - 1 : TE + ty;
+                    bp = tx > 0 ? (e - 1) * LX : (2 * TE + ty) * LX;
+                    sn = tx < txe - 1 ? e + 1 : TE + TY + ty;
+                    bn = tx < txe - 1 ? (e + 1) * LX : (2 * TE + TY + ty) * LX;
+                }
+                else
+                {
+                    sp = ty > 0 ? e - TX : TE + 2 * TY + tx;
+                    bp = ty > 0 ? (TE + e - TX) * LX : (2 * TE + 2 * TY + tx) * LX;
+                    sn = ty < tye - 1 ? e + TX : TE + 2 * TY + TX + tx;
+                    bn = ty < tye - 1 ? (TE + e + TX) * LX : (2 * TE + 2 * TY + TX + tx) * LX;
+                }
+                const double b0 = sB[bp + li], b1 = sB[(dir * TE + e) * LX + li], b2 = sB[bn + li];
+                // ShockSensor::detect_shock (filter.hpp:654-678)
+                double cg0 = a.gam[0] / ((1.0e-6 + b0) * (1.0e-6 + b0));
+                double cg1 = a.gam[1] / ((1.0e-6 + b1) * (1.0e-6 + b1));
+                double cg2 = a.gam[2] / ((1.0e-6 + b2) * (1.0e-6 + b2));
+                const double ws = cg0 + cg1 + cg2;
+                cg0 /= ws;
+                cg1 /= ws;
+                cg2 /= ws;
+                const double num = sensor_pow(fabs(cg0 / a.gam[0] - 1.0), a.theta) +
+                                   sensor_pow(fabs(cg1 / a.gam[1] - 1.0), a.theta) +
+                                   sensor_pow(fabs(cg2 / a.gam[2] - 1.0), a.theta);
+                const double r_j = num * a.one_over_norm;
+                if (fabs(r_j) >= a.threshold)
+                {
+                    // WENOLimiter::apply_weno_scalar (filter.hpp:519-544)
+                    double pv[N], nv[N];
+                    line_vals(sp, dir, li, pv);
+                    line_vals(sn, dir, li, nv);
+                    double ap = 0.0, ac = 0.0, an = 0.0;
+#pragma unroll
+                    for (int i = 0; i < N; ++i)
+                    {
+                        ap += a.w[i] * pv[i];
+                        ac += a.w[i] * cv[i];
+                        an += a.w[i] * nv[i];
+                    }
+                    ap *= 0.5;
+                    ac *= 0.5;
+                    an *= 0.5;
+#pragma unroll
+                    for (int i = 0; i < N; ++i) o[i] = cg0 * (pv[i] - ap + ac) + cg1 * cv[i] + cg2 * (nv[i] - an + ac);
+                }
+                else
+                {
+#pragma unroll
+                    for (int i = 0; i < N; ++i) o[i] = cv[i];
+                }
+            }
+            else
+            {
+                // SpectralFilter::apply_filter (filter.hpp:425-445)
+#pragma unroll
+                for (int r = 0; r < N; ++r)
+                {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int c = 0; c < N; ++c) acc += a.F[r * N + c] * cv[c];
+                    o[r] = acc;
+                }
+            }
+            const int eq = li % 4, m = li / 4;
+            double* dst = sX + e * ND + eq;
+#pragma unroll
+            for (int t = 0; t < N; ++t)
+            {
+                const int node = dir == 0 ? m * N + t : t * N + m;
+                dst[node * 4] = dir == 0 ? o[t] : 0.5 * (dst[node * 4] + o[t]);
+            }
+        }
+        __syncthreads();
+    }
+
+    // store the tile
+    for (int q = tid; q < TE * (ND / 2); q += kThreads)
+    {
+        const int e = q / (ND / 2), k = q % (ND / 2), tx = e % TX, ty = e / TX;
+        if (tx >= txe || ty >= tye) continue;
+        reinterpret_cast<double2*>(a.dst + (int64_t(j0 + ty) * a.Nx + (i0 + tx)) * ND)[k] =
+            reinterpret_cast<const double2*>(sX + e * ND)[k];
     }
 }
 
@@ -190,10 +386,21 @@ template <int N> cudaError_t launch_stab_n(const StabArgs& a, cudaStream_t s)
 {
     if (a.dim == 2)
     {
-        constexpr int LPE = 8 * N;
-        constexpr int E = (kThreads / LPE) > 0 ? kThreads / LPE : 1;
-        const int64_t nel = int64_t(a.Nx) * a.Ny;
-        stab2d_kernel<N><<<unsigned((nel + E - 1) / E), kThreads, 0, s>>>(a);
+        using T = StabTile<N>;
+        auto kern = stab2d_tile_kernel<N>;
+        // the shared-memory opt-in is per device: set it once on each device that launches
+        static bool attr_done[64] = {};
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (dev < 0 || dev >= 64 || !attr_done[dev])
+        {
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(T::bytes));
+            if (e != cudaSuccess) return e;
+            if (dev >= 0 && dev < 64) attr_done[dev] = true;
+        }
+        dim3 grid((a.Nx + T::TX - 1) / T::TX, (a.Ny + T::TY - 1) / T::TY);
+        kern<<<grid, kThreads, T::bytes, s>>>(a);
     }
     else
     {
