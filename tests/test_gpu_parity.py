@@ -151,7 +151,8 @@ def test_change_of_variables_2d(name, cuda):
 
 
 @pytest.mark.parametrize("stab", ["filter", "weno", "both"])
-@pytest.mark.parametrize("name", ["cart_ideal_rusanov_p3", "cart_vdw_rusanov_p5_perx", "sinewarp_hllc_p4_periodic"])
+@pytest.mark.parametrize("name", ["cart_ideal_rusanov_p3", "cart_vdw_rusanov_p5_perx", "sinewarp_hllc_p4_periodic",
+                                  "cart_ideal_hllc_p7", "cart_vdw_hllc_p8_periodic"])
 def test_post_step_2d(name, stab, cuda):
     kw = dict(CASES_2D[name])
     kw.update(apply_filter=stab in ("filter", "both"), apply_weno=stab in ("weno", "both"), threshold=0.3)
