@@ -115,6 +115,23 @@ __global__ void __launch_bounds__(kInvThreads) block_inverse_kernel(const double
     for (int q = tid; q < n * n; q += kInvThreads) inv[base + q] = static_cast<float>(sA[q]);
 }
 
+// Row i of B v for an n x n FP32 block stored column-major (entry (i, j) at j n + i):
+// four partial sums, so four loads and four FMA chains are in flight per thread.
+__device__ __forceinline__ double block_row(const float* __restrict__ B, const double* v, int n, int i)
+{
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int j = 0;
+    for (; j + 3 < n; j += 4)
+    {
+        a0 = fma(static_cast<double>(__ldg(B + int64_t(j) * n + i)), v[j], a0);
+        a1 = fma(static_cast<double>(__ldg(B + int64_t(j + 1) * n + i)), v[j + 1], a1);
+        a2 = fma(static_cast<double>(__ldg(B + int64_t(j + 2) * n + i)), v[j + 2], a2);
+        a3 = fma(static_cast<double>(__ldg(B + int64_t(j + 3) * n + i)), v[j + 3], a3);
+    }
+    for (; j < n; ++j) a0 = fma(static_cast<double>(__ldg(B + int64_t(j) * n + i)), v[j], a0);
+    return (a0 + a1) + (a2 + a3);
+}
+
 // z_e = inv_e r_e for every element e: one CTA per element, thread i owns row i.
 __global__ void block_apply_kernel(const float* __restrict__ inv, const double* __restrict__ r, double* __restrict__ z, int n)
 {
@@ -123,12 +140,7 @@ __global__ void block_apply_kernel(const float* __restrict__ inv, const double* 
     for (int j = threadIdx.x; j < n; j += blockDim.x) sr[j] = r[e * n + j];
     __syncthreads();
     const float* B = inv + e * int64_t(n) * n;
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
-    {
-        double acc = 0.0;
-        for (int j = 0; j < n; ++j) acc = fma(static_cast<double>(__ldg(B + int64_t(j) * n + i)), sr[j], acc);
-        z[e * n + i] = acc;
-    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) z[e * n + i] = block_row(B, sr, n, i);
 }
 
 // Off-diagonal blocks (slots 1-4 of each element's five) to FP32, packed four per element.
@@ -174,19 +186,14 @@ __global__ void block_gs_kernel(const float* __restrict__ inv, const float* __re
         double acc = 0.0;
         if (phase > 0)
             for (int s = 0; s < 4; ++s)
-            {
-                if (nbi[s] < 0) continue;
-                const float* B = off + (e * 4 + s) * int64_t(n) * n;
-                for (int j = 0; j < n; ++j) acc = fma(static_cast<double>(__ldg(B + int64_t(j) * n + i)), nbv[s * n + j], acc);
-            }
+                if (nbi[s] >= 0) acc += block_row(off + (e * 4 + s) * int64_t(n) * n, nbv + s * n, n, i);
         t[i] = phase == 0 ? r[e * n + i] : phase == 1 ? r[e * n + i] - acc : acc;
     }
     __syncthreads();
     const float* Bi = inv + e * int64_t(n) * n;
     for (int i = threadIdx.x; i < n; i += blockDim.x)
     {
-        double acc = 0.0;
-        for (int j = 0; j < n; ++j) acc = fma(static_cast<double>(__ldg(Bi + int64_t(j) * n + i)), t[j], acc);
+        const double acc = block_row(Bi, t, n, i);
         z[e * n + i] = phase == 2 ? z[e * n + i] - acc : acc;
     }
 }
