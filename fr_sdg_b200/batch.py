@@ -141,7 +141,7 @@ class BatchedInstances:
                 st = self.streams[k % len(self.streams)]
                 st.wait_stream(cur)
                 with torch.cuda.stream(st):
-                    graphs.append(it._capture(U, dt, steps_per_graph))
+                    graphs.append(it.capture(U, dt, steps_per_graph))
             for st in self.streams:
                 cur.wait_stream(st)
             torch.cuda.synchronize(self.device)

@@ -142,7 +142,7 @@ class Integrator:
         faces = range(4) if cfg.dim == 2 else (A.LEFT, A.RIGHT)
         return any(cfg.bc[f].kind == A.BC_VORTEX for f in faces)
 
-    def _capture(self, U: torch.Tensor, dt: float, steps: int) -> torch.cuda.CUDAGraph:
+    def capture(self, U: torch.Tensor, dt: float, steps: int) -> torch.cuda.CUDAGraph:
         """`steps` full steps of size dt captured into one CUDA graph that updates U in
         place (kernel launches and device copies only: no allocation, no sync).  The
         capture runs on a side stream ordered after the current one."""
@@ -184,7 +184,7 @@ class Integrator:
         t, k = t0, 0
         if graph and n_full >= steps_per_graph and not self.time_dependent() and self.before is None and (
                 monitor is None or not monitor.every_step_matters):
-            g = self._capture(U, dt, steps_per_graph)
+            g = self.capture(U, dt, steps_per_graph)
             for _ in range(n_full // steps_per_graph):
                 g.replay()
                 for _ in range(steps_per_graph):
