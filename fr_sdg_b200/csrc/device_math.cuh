@@ -134,16 +134,6 @@ __device__ __forceinline__ cplx s_wrap_positive(cplx r)
 
 template <class S> __device__ __forceinline__ S s_select(bool c, S a, S b) { return c ? a : b; }
 
-// Health word update: count the calling lanes whose flag is set with one atomic per
-// warp (a state that went non-finite everywhere would otherwise serialise every
-// node of every launch on one counter).
-__device__ __forceinline__ void count_bad(unsigned long long* counter, bool bad)
-{
-    const unsigned active = __activemask();
-    const unsigned m = __ballot_sync(active, bad);
-    if (m && counter && (threadIdx.x & 31) == unsigned(__ffs(m) - 1)) atomicAdd(counter, static_cast<unsigned long long>(__popc(m)));
-}
-
 template <class S> struct scalar_traits;
 template <> struct scalar_traits<double>
 {

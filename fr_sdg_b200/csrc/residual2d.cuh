@@ -432,7 +432,6 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
             hrec = r;
         }
     }
-    unsigned nbad = 0;  // tile nodes with a non-positive or non-finite density
     for (int q = tid; q < TE * NN; q += BT)
     {
         const int e = q / NN, node = q % NN, tx = e % TX, ty = e / TX, k = node % N, l = node / N;
@@ -446,7 +445,7 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
 #pragma unroll
                 for (int eq = 0; eq < 4; ++eq) sSeed[(e * 4 + eq) * NN + node] = s_im(s[eq]);
             }
-            nbad += !(s_re(s[0]) > 0.0);
+            if (!(s_re(s[0]) > 0.0) && a.bad) atomicAdd(a.bad, 1ull);
             const NodePrim<S> pr = node_prim<GAS>(g, s[0], s[1], s[2], s[3]);
             const S rEp = s[3] + pr.p;
             const S ruv = s[1] * pr.v;
@@ -477,12 +476,6 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
         make_record<GAS>(g, hs, pr, rec);
 #pragma unroll
         for (int fld = 0; fld < RF_N; ++fld) sRec[fld * NREC + hrec] = rec[fld];
-    }
-    if (a.bad)
-    {
-        // one atomic per warp (every lane of the block gets here)
-        const unsigned tot = __reduce_add_sync(0xffffffffu, nbad);
-        if (tot && (tid & 31) == 0) atomicAdd(a.bad, static_cast<unsigned long long>(tot));
     }
     __syncthreads();
 
