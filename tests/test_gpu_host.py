@@ -1,6 +1,5 @@
 """GPU: the host-vector entry point (frsdg_rhs_host) returns the device rhs bit for bit
 -- pipelined over row chunks on 2D meshes (periodic and not), in one piece in 1D."""
-import numpy as np
 import pytest
 import torch
 

@@ -6,7 +6,6 @@ import pytest
 import torch
 
 from fr_sdg_b200 import FRSolver
-from fr_sdg_b200 import _abi as A
 from fr_sdg_b200.integrate import Integrator, cfl_time_step, l2_error, node_jacobian
 from fr_sdg_b200.workloads import blast_large, exact_vortex, node_coords, pack2d, sod1d, vortex_curved
 from oracle.oracle import Oracle

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 import torch
 
-from fr_sdg_b200 import FRSolver, FrsdgError
+from fr_sdg_b200 import FRSolver
 from fr_sdg_b200.integrate import Integrator, cfl_time_step
 from fr_sdg_b200.petsc_io import SolutionMonitor, pack_record
 from fr_sdg_b200.workloads import sod1d, vortex_curved

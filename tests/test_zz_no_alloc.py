@@ -10,7 +10,6 @@ so that pytest collects it last.
 """
 import ctypes as C
 
-import numpy as np
 import pytest
 import torch
 
