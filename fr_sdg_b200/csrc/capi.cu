@@ -326,7 +326,8 @@ int frsdg_create(const frsdg_config* cfg, frsdg_handle** out)
     const bool per_x = cfg->bc[FRSDG_LEFT].kind == FRSDG_BC_PERIODIC;
     const bool per_y = cfg->dim == 2 && cfg->bc[FRSDG_TOP].kind == FRSDG_BC_PERIODIC;
 
-    if ((rc = upload(&h->d_bad, std::vector<unsigned long long>{0ull})))
+    rc = upload(&h->d_bad, std::vector<unsigned long long>(1, 0ull));
+    if (rc != FRSDG_OK)
     {
         free_handle(h);
         return rc;
@@ -605,7 +606,7 @@ int frsdg_rk_stage(frsdg_handle* h, double t, const double* Us, const double* A,
     if (out == Us) return fail(FRSDG_ERR_ARG, "frsdg_rk_stage: out must not alias Us");
     if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(acc)) & 15)
         return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
-    StageArgs st{A, B, acc, alpha, beta, gamma, delta};
+    StageArgs st{A, B, acc, alpha, beta, gamma, delta, nullptr};
     return run_residual(h, MODE_STAGE, t, Us, nullptr, out, stream, &st);
 }
 
