@@ -75,6 +75,7 @@ SIGNATURES = {
     "frsdg_jac_blocks5": (C.c_int, [_P, _D, _D, _P, _P, _P]),
     "frsdg_pc_setup_gs": (C.c_int, [_P, _D, _D, _P, _P]),
     "frsdg_post_step": (C.c_int, [_P, _P, _P]),
+    "frsdg_post_step_to": (C.c_int, [_P, _P, _P, _P]),
     "frsdg_post_step_static": (C.c_int, [C.POINTER(frsdg_config), _P, _P]),
     "frsdg_prim_to_cons": (C.c_int, [_P, _P, _P, _P]),
     "frsdg_rhs_host": (C.c_int, [_P, _D, _P, _P, _P]),

@@ -862,6 +862,33 @@ int frsdg_post_step(frsdg_handle* h, double* U, void* stream)
     return FRSDG_OK;
 }
 
+int frsdg_post_step_to(frsdg_handle* h, const double* src, double* dst, void* stream)
+{
+    if (!h || !src || !dst) return fail(FRSDG_ERR_ARG, "null argument");
+    if ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15)
+        return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
+    if (src == dst) return fail(FRSDG_ERR_ARG, "frsdg_post_step_to: src and dst must not alias");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    h->last = s;
+    if (!h->cfg.apply_filter && !h->cfg.apply_weno)
+    {
+        cudaError_t e = cudaMemcpyAsync(dst, src, sizeof(double) * local_ntot(h), cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return cuda_fail(e, "post-step copy");
+        return FRSDG_OK;
+    }
+    StabArgs a = h->st;
+    a.src = src;
+    a.dst = dst;
+    if (h->win_rows)
+    {
+        a.Ny = h->win_rows;
+        a.per_y = 0;
+    }
+    cudaError_t e = launch_stab(h->n, a, s);
+    if (e != cudaSuccess) return cuda_fail(e, "post-step launch");
+    return FRSDG_OK;
+}
+
 int frsdg_prim_to_cons(frsdg_handle* h, const double* prim, double* cons, void* stream)
 {
     if (!h || !prim || !cons) return fail(FRSDG_ERR_ARG, "null argument");

@@ -121,20 +121,24 @@ class Integrator:
             return self._step_mixed(U, t, dt)
         s = self.s
         b1, b2, b3 = self._buffers(U)[:3]
+        # with a limiter, the last stage goes to a free buffer and the limiter writes U
+        # from it (frsdg_post_step_to: no device copy of the state)
         if self.scheme == "ssprk3":
+            last = b3 if self.stabilise else U
             self._rk(t, U, b1, gamma=dt, a=U, alpha=1.0)
             self._rk(t + dt, b1, b2, gamma=0.25 * dt, a=U, alpha=0.75, b=b1, beta=0.25)
-            self._rk(t + 0.5 * dt, b2, U, gamma=2.0 * dt / 3.0, a=U, alpha=1.0 / 3.0, b=b2, beta=2.0 / 3.0)
+            self._rk(t + 0.5 * dt, b2, last, gamma=2.0 * dt / 3.0, a=U, alpha=1.0 / 3.0, b=b2, beta=2.0 / 3.0)
         else:
+            last = b2 if self.stabilise else U
             b3.copy_(U)
             self._rk(t, U, b1, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 6.0)
             self._rk(t + 0.5 * dt, b1, b2, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
             self._rk(t + 0.5 * dt, b2, b1, gamma=dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
-            self._rk(t + dt, b1, U, gamma=dt / 6.0, a=b3, alpha=1.0)
+            self._rk(t + dt, b1, last, gamma=dt / 6.0, a=b3, alpha=1.0)
         if self.stabilise:
             if self.before is not None:
-                self.before(U)
-            s.apply_stabilization(U)
+                self.before(last)
+            s.apply_stabilization_to(last, U)
 
     def time_dependent(self) -> bool:
         """Whether the residual reads t (the exact-vortex boundary kind)."""

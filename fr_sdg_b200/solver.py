@@ -160,6 +160,11 @@ class FRSolver:
         self._check_vec(U)
         A.check(self._lib.frsdg_post_step(self._h, _ptr(U), _stream()), "frsdg_post_step")
 
+    def apply_stabilization_to(self, src: torch.Tensor, dst: torch.Tensor) -> None:
+        """dst = limit(src) without touching src (no counterpart in the reference)."""
+        self._check_vec(src, dst)
+        A.check(self._lib.frsdg_post_step_to(self._h, _ptr(src), _ptr(dst), _stream()), "frsdg_post_step_to")
+
     def primitive_to_conservative(self, inp: torch.Tensor, out: torch.Tensor) -> None:
         self._check_vec(inp, out)
         A.check(self._lib.frsdg_prim_to_cons(self._h, _ptr(inp), _ptr(out), _stream()), "frsdg_prim_to_cons")

@@ -247,6 +247,13 @@ int frsdg_rk_stage(frsdg_handle* h, double t, const double* Us, const double* A,
  * shock sensor): PetscSolver::apply_stabilization (petsc_solver_impl.hpp:683-702). */
 int frsdg_post_step(frsdg_handle* h, double* U, void* stream);
 
+/* Out-of-place post-step: dst = limit(src), src left unchanged; src and dst must not
+ * alias (frsdg_post_step on dst with src's values gives the same result).  It has no
+ * counterpart in the reference: a time integrator that writes its last stage to a
+ * separate buffer limits it into the state directly, without the device copy of the
+ * state that the in-place call makes for the WENO limiter. */
+int frsdg_post_step_to(frsdg_handle* h, const double* src, double* dst, void* stream);
+
 /* cons = M(prim): PetscSolver::primitive_to_conservative (petsc_solver_impl.hpp:719-727). */
 int frsdg_prim_to_cons(frsdg_handle* h, const double* prim, double* cons, void* stream);
 

@@ -234,3 +234,23 @@ def test_free_stream_preserved_large(cuda):
         R = torch.empty_like(U)
         s.residual_kernel(0.0, U, R)
         assert R.abs().max().item() < 1e-11
+
+
+@pytest.mark.parametrize("stab", ["filter", "weno"])
+def test_post_step_to_equals_in_place(stab, cuda):
+    """frsdg_post_step_to (src -> dst, no device copy) gives the in-place post-step's
+    result bit for bit and leaves src unchanged; aliasing src and dst is refused."""
+    kw = dict(CASES_2D["cart_vdw_rusanov_p5_perx"])
+    kw.update(apply_filter=stab == "filter", apply_weno=stab == "weno", threshold=0.3)
+    cfg = _cfg2d(**kw)
+    U = _dev(random_state(cfg, seed=37), cuda)
+    with FRSolver(cfg) as s:
+        ref = U.clone()
+        s.apply_stabilization(ref)
+        src = U.clone()
+        dst = torch.full_like(U, float("nan"))
+        s.apply_stabilization_to(src, dst)
+        torch.cuda.synchronize()
+        assert torch.equal(dst, ref)
+        assert torch.equal(src, U)
+        assert A.lib().frsdg_post_step_to(s._h, src.data_ptr(), src.data_ptr(), None) == A.ERR_ARG
