@@ -11,6 +11,7 @@
 // In 2D each element gets 1/2 (x-line result + y-line result).  Neighbours across
 // a non-periodic boundary are zero (the never-written ghost entries of a PETSc
 // local vector).
+#include "device_math.cuh"
 #include "frsdg_internal.hpp"
 #include "stab.hpp"
 
@@ -150,6 +151,7 @@ template <int N> __global__ void __launch_bounds__(kThreads, N <= 6 ? 3 : 1) sta
     const int txe = min(TX, a.Nx - i0), tye = min(TY, a.Ny - j0);
     const bool weno = a.apply_weno && !a.apply_filter;
     const int nslot = weno ? T::NSLOT : TE;
+    const double igam0 = 1.0 / a.gam[0], igam1 = 1.0 / a.gam[1], igam2 = 1.0 / a.gam[2];
 
     // global element of a slot, or -1 (outside the tile or a zero ghost across a
     // non-periodic boundary)
@@ -258,16 +260,18 @@ template <int N> __global__ void __launch_bounds__(kThreads, N <= 6 ? 3 : 1) sta
                 }
                 const double b0 = sB[bp + li], b1 = sB[(dir * TE + e) * LX + li], b2 = sB[bn + li];
                 // ShockSensor::detect_shock (filter.hpp:654-678)
-                double cg0 = a.gam[0] / ((1.0e-6 + b0) * (1.0e-6 + b0));
-                double cg1 = a.gam[1] / ((1.0e-6 + b1) * (1.0e-6 + b1));
-                double cg2 = a.gam[2] / ((1.0e-6 + b2) * (1.0e-6 + b2));
-                const double ws = cg0 + cg1 + cg2;
-                cg0 /= ws;
-                cg1 /= ws;
-                cg2 /= ws;
-                const double num = sensor_pow(fabs(cg0 / a.gam[0] - 1.0), a.theta) +
-                                   sensor_pow(fabs(cg1 / a.gam[1] - 1.0), a.theta) +
-                                   sensor_pow(fabs(cg2 / a.gam[2] - 1.0), a.theta);
+                // divisions as reciprocals and products (within a few ulps of the
+                // reference's quotients; the 1/gamma_k are shared by every line)
+                double cg0 = a.gam[0] * s_rcp((1.0e-6 + b0) * (1.0e-6 + b0));
+                double cg1 = a.gam[1] * s_rcp((1.0e-6 + b1) * (1.0e-6 + b1));
+                double cg2 = a.gam[2] * s_rcp((1.0e-6 + b2) * (1.0e-6 + b2));
+                const double iws = s_rcp(cg0 + cg1 + cg2);
+                cg0 *= iws;
+                cg1 *= iws;
+                cg2 *= iws;
+                const double num = sensor_pow(fabs(cg0 * igam0 - 1.0), a.theta) +
+                                   sensor_pow(fabs(cg1 * igam1 - 1.0), a.theta) +
+                                   sensor_pow(fabs(cg2 * igam2 - 1.0), a.theta);
                 const double r_j = num * a.one_over_norm;
                 if (fabs(r_j) >= a.threshold)
                 {
