@@ -79,8 +79,10 @@ def gmres(matvec, precond, b: torch.Tensor, restart: int = 30, rtol: float = 1e-
             w -= V[: j + 1].T @ h
             h2 = V[: j + 1] @ w
             w -= V[: j + 1].T @ h2
-            h = (h + h2).cpu().numpy()
-            hn = float(torch.linalg.vector_norm(w))
+            # the new Hessenberg column and ||w|| in one device-to-host read
+            hn_dev = torch.linalg.vector_norm(w).reshape(1)
+            col = torch.cat((h + h2, hn_dev)).cpu().numpy()
+            h, hn = col[:-1], float(col[-1])
             H[: j + 1, j] = h
             H[j + 1, j] = hn
             for i in range(j):
@@ -98,7 +100,7 @@ def gmres(matvec, precond, b: torch.Tensor, restart: int = 30, rtol: float = 1e-
             rel = abs(g[j + 1]) / bnorm
             if rel <= rtol or hn == 0.0 or total >= max_iter:
                 break
-            V[j + 1] = w / hn
+            torch.div(w, hn_dev, out=V[j + 1])
         y = np.zeros(k)
         for i in range(k - 1, -1, -1):
             y[i] = (g[i] - H[i, i + 1:k] @ y[i + 1:k]) / H[i, i]
