@@ -374,6 +374,28 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
     const int txe = min(TX, Nx - i0), tye = min(TY, a.row_end - j0);
     const GasParams g = a.gas;
 
+    if constexpr (!T::JVP)
+    {
+        // Epilogue operands (RK stage: A and B; IFunction: U_t): pull the tile's lines
+        // into L2 first, so that their reads after the face phase do not wait on HBM
+        // (prefetches are hints; measured: SSP-RK3 stage on the 1024^2 p5 blast 1.95 ->
+        // 1.74 ms)
+        if (a.mode == MODE_STAGE || a.mode == MODE_IFUNC)
+        {
+            constexpr int LROW = (TX * ND * int(sizeof(double)) + 127) / 128;  // 128-byte lines per tile row
+            const int lrow = (txe * ND * int(sizeof(double)) + 127) / 128;
+            const double* b0 = a.mode == MODE_STAGE ? a.st.A : a.W;
+            const double* b1 = a.mode == MODE_STAGE ? a.st.B : nullptr;
+            for (int q = tid; q < 2 * TY * LROW; q += BT)
+            {
+                const int which = q / (TY * LROW), r = q % (TY * LROW), ty = r / LROW, ln = r % LROW;
+                const double* base = which ? b1 : b0;
+                if (base && ty < tye && ln < lrow)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(base + (int64_t(j0 + ty) * Nx + i0) * ND + ln * 16));
+            }
+        }
+    }
+
     // ---- P1: nodes of the tile; the halo traces (x-left, x-right per tile row,
     // y-bottom, y-top per tile column) are fetched first so their latency overlaps
     static_assert(T::NHALO <= BT, "one halo node per thread");
