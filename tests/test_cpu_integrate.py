@@ -1,0 +1,90 @@
+"""CPU: the host logic of the explicit integrator -- stage sequences, the clipped final
+step and the solution-monitor schedule -- over a stand-in solver whose right-hand side
+is rhs(U) = -U (so the exact solution is U0 exp(-t)) and whose limiter is the identity."""
+from __future__ import annotations
+
+import math
+from types import SimpleNamespace
+
+import pytest
+import torch
+
+from fr_sdg_b200.integrate import Integrator
+
+
+class DecaySolver:
+    """The rk_stage / apply_stabilization contract of FRSolver for dU/dt = -U."""
+
+    def __init__(self, limiter: bool):
+        self.cfg = SimpleNamespace(apply_filter=int(limiter), apply_weno=0, dim=2, cond_sys=0,
+                                   bc=[SimpleNamespace(kind=0) for _ in range(4)])
+        self.stages = 0
+        self.limits = 0
+
+    def rk_stage(self, t, Us, out, gamma, a=None, alpha=0.0, b=None, beta=0.0, acc=None, delta=0.0):
+        assert out.data_ptr() != Us.data_ptr()
+        v = -Us.clone()
+        o = torch.zeros_like(Us)
+        if a is not None:
+            o = alpha * a
+        if b is not None:
+            o = o + beta * b
+        if acc is not None:
+            acc += delta * v
+        out.copy_(o + gamma * v)
+        self.stages += 1
+
+    def apply_stabilization(self, U):
+        self.limits += 1
+
+    def apply_stabilization_to(self, src, dst):
+        assert src.data_ptr() != dst.data_ptr()
+        dst.copy_(src)
+        self.limits += 1
+
+
+@pytest.mark.parametrize("scheme,order", [("ssprk3", 3), ("rk4", 4)])
+@pytest.mark.parametrize("limiter", [False, True])
+def test_stage_sequences_converge_at_their_order(scheme, order, limiter):
+    errs = []
+    for n in (20, 40):
+        s = DecaySolver(limiter)
+        U = torch.ones(8, dtype=torch.float64)
+        st = Integrator(s, scheme).run(U, 1.0 / n, t_end=1.0)
+        assert st.steps == n and abs(st.t - 1.0) < 1e-14
+        assert s.stages == n * (3 if scheme == "ssprk3" else 4)
+        assert s.limits == (n if limiter else 0)
+        errs.append(float((U - math.exp(-1.0)).abs().max()))
+    rate = math.log2(errs[0] / errs[1])
+    assert abs(rate - order) < 0.2, (errs, rate)
+
+
+def test_clipped_final_step_and_monitor_schedule():
+    """t_end = 10.5 dt: ten full steps and one clipped step of dt/2; a monitor with
+    interval 4 sees steps 0, 4, 8 and the final step 11."""
+    s = DecaySolver(limiter=True)
+    U = torch.ones(4, dtype=torch.float64)
+    dt = 0.05
+    seen = []
+
+    class Monitor:
+        every_step_matters = True
+
+        def __call__(self, step, t, V, final):
+            if step % 4 == 0 or final:
+                seen.append((step, round(t / dt, 9), final))
+
+    st = Integrator(s, "ssprk3").run(U, dt, t_end=10.5 * dt, monitor=Monitor())
+    assert st.steps == 11 and abs(st.t - 10.5 * dt) < 1e-15
+    assert seen == [(0, 0.0, False), (4, 4.0, False), (8, 8.0, False), (11, 10.5, True)]
+    # the clipped step is the exact SSP-RK3 map with h = dt / 2 after ten full steps
+    g = lambda h: 1 - h + h * h / 2 - h ** 3 / 6
+    assert abs(float(U[0]) - g(dt) ** 10 * g(dt / 2)) < 1e-15
+
+
+def test_before_stage_hook_sees_every_stage_input_and_the_limiter_input():
+    s = DecaySolver(limiter=True)
+    U = torch.ones(4, dtype=torch.float64)
+    calls = []
+    Integrator(s, "ssprk3", before_stage=lambda V: calls.append(V.data_ptr())).step(U, 0.0, 0.1)
+    assert len(calls) == 4 and calls[0] == U.data_ptr() and calls[3] != U.data_ptr()
