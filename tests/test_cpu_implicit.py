@@ -112,3 +112,54 @@ def test_coarse_colouring_is_distance_two():
             assert len(set(cols)) == len(cols)
             match = [b * gx + a for a, b in hood if int(col[b, a]) == c]
             assert int(nb[k]) == (match[0] if match else -1)
+
+
+class _PseudoTimeModel:
+    """Stand-ins for march_to_steady: a 'solver' whose residual norm is the first entry
+    of U, and a 'Newton step' that multiplies it by 1 / (1 + dt) -- or blows it up when
+    dt exceeds blow_dt (a step the march must reject)."""
+
+    def __init__(self, blow_dt: float):
+        self.blow_dt = blow_dt
+        self.dts = []
+
+    # solver side
+    def residual_kernel(self, t, U, R):
+        R.zero_()
+        R[0] = U[0]
+
+    def status(self):
+        return 0
+
+    # Newton side
+    def step(self, U, t, dt):
+        from fr_sdg_b200.implicit import NewtonStats
+
+        self.dts.append(dt)
+        U[0] = U[0] * (1e6 if dt > self.blow_dt else 1.0 / (1.0 + dt))
+        return NewtonStats(1, 3)
+
+
+def test_march_rejects_growth_and_caps_the_time_step():
+    from fr_sdg_b200.implicit import march_to_steady
+
+    m = _PseudoTimeModel(blow_dt=50.0)
+    U = torch.ones(4, dtype=torch.float64)
+    st = march_to_steady(m, U, dt0=0.5, drop=1e-10, max_steps=200, newton=m, max_growth=3.0, reject_growth=1.5)
+    assert st.residual_drop <= 1e-10
+    # every attempt above blow_dt grew the residual 1e6-fold and was rejected (dt / 4)
+    assert st.rejected == sum(1 for dt in m.dts if dt > 50.0) and st.rejected > 0
+    for a, b in zip(m.dts, m.dts[1:]):
+        assert b <= 3.0 * a + 1e-12 or b == a / 4  # growth capped, or a rejection's quarter step
+    assert st.gmres_iterations == 3 * len(m.dts)  # rejected attempts' Krylov work counts too
+
+
+def test_march_without_rejection_rule_accepts_growth():
+    from fr_sdg_b200.implicit import march_to_steady
+
+    m = _PseudoTimeModel(blow_dt=1e9)
+    U = torch.ones(4, dtype=torch.float64)
+    st = march_to_steady(m, U, dt0=0.5, drop=1e-8, max_steps=100, newton=m)
+    assert st.rejected == 0 and st.residual_drop <= 1e-8
+    # switched evolution relaxation: dt_k = dt0 / drop_k
+    assert all(abs(b - min(0.5 / d, 1e6)) < 1e-9 * b for b, d in zip(m.dts[1:], st.history[1:]))
