@@ -1,4 +1,5 @@
-"""CPU: row-block partitions and the ghost-row exchange (gloo, 2 and 3 ranks)."""
+"""CPU: row-block partitions, the ghost-row exchange, the integrator's ghost hook and the
+global wave-speed maximum (gloo, 2 and 3 ranks)."""
 import os
 import socket
 
@@ -7,7 +8,7 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from fr_sdg_b200.partition import exchange_ghost_rows, row_blocks, scatter_rows
+from fr_sdg_b200.partition import exchange_ghost_rows, ghost_hook, global_max, row_blocks, scatter_rows
 
 
 @pytest.mark.parametrize("ny,ranks,periodic", [(10, 1, False), (10, 1, True), (10, 2, False), (10, 2, True),
@@ -52,7 +53,19 @@ def _worker(rank, ws, port, ny, periodic, q):
             got[-1] = -1.0
         got = got.reshape(-1)
         exchange_ghost_rows(got, blk, nx * nd)
-        q.put((rank, bool(torch.equal(got, want))))
+        ok = bool(torch.equal(got, want))
+        # the integrator's stage hook does the same refresh
+        got2 = want.clone().view(blk.rows, nx * nd)
+        if blk.ghost_below:
+            got2[0] = -2.0
+        if blk.ghost_above:
+            got2[-1] = -2.0
+        got2 = got2.reshape(-1)
+        ghost_hook(blk, nx * nd)(got2)
+        ok = ok and bool(torch.equal(got2, want))
+        # the CFL wave speed is the max over the ranks
+        ok = ok and global_max(rank + 0.5, "cpu") == ws - 0.5
+        q.put((rank, ok))
     finally:
         dist.destroy_process_group()
 
