@@ -88,3 +88,29 @@ def test_before_stage_hook_sees_every_stage_input_and_the_limiter_input():
     calls = []
     Integrator(s, "ssprk3", before_stage=lambda V: calls.append(V.data_ptr())).step(U, 0.0, 0.1)
     assert len(calls) == 4 and calls[0] == U.data_ptr() and calls[3] != U.data_ptr()
+
+
+def test_cfl_time_step_uniform_states():
+    """dt = CFL (L/N) / max(|v| + c): ideal gas c^2 = gamma p / rho; Van der Waals
+    c^2 = [gamma (gamma-1)(e + a rho) + (gamma-1) a rho (2 - b rho)] / (1 - b rho)^2 - 2 a rho
+    (gas_models.hpp:89-158), from the state's specific internal energy."""
+    from fr_sdg_b200.integrate import cfl_time_step
+    from fr_sdg_b200.workloads import make_config, pack2d, rhoE
+
+    n_nodes = 3 * 2 * 16
+    rho, u, v, p, g = 1.2, 0.3, -0.4, 0.9, 1.4
+    for gas, (a, b) in (("ideal", (0.0, 0.0)), ("vdw", (0.05, 0.02))):
+        cfg = make_config(dim=2, p=3, n_elems=(3, 2), box=(0.6, 0.4), gas=gas, vdw=(a, b))
+        ones = torch.ones(n_nodes, dtype=torch.float64)
+        E = rhoE(gas, g, a, b, rho * ones, (u * u + v * v) * ones, p * ones)
+        U = pack2d(rho * ones, rho * u * ones, rho * v * ones, E)
+        dt = cfl_time_step(cfg, U, 0.5)
+        if gas == "ideal":
+            c = math.sqrt(g * p / rho)
+        else:
+            e = float(E[0]) / rho - 0.5 * (u * u + v * v)
+            cov = 1.0 - b * rho
+            c = math.sqrt((g * (g - 1) * (e + a * rho) + (g - 1) * a * rho * (2 - b * rho)) / (cov * cov) - 2 * a * rho)
+            # the state's pressure from the same gas law
+            assert abs((g - 1) * rho * (e + a * rho) / cov - a * rho * rho - p) < 1e-12
+        assert abs(dt - 0.5 * 0.2 / (math.hypot(u, v) + c)) < 1e-12 * dt, gas
