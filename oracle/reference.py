@@ -1,0 +1,151 @@
+"""ctypes wrapper of oracle/_ref/libfrsdg_ref.so: fr_sdg's own hot-path code
+(include/*.hpp of the reference, compiled by oracle/ref_build.py against the
+stand-ins of oracle/ref_shim) behind the same calls as oracle.Oracle.
+
+TEST INFRASTRUCTURE ONLY: the tests use it to pin the restated oracle to the
+reference, tests/golden/gen_ref_golden.py to freeze reference outputs as
+fixtures, and bench.py's reference arm to time the reference's own residual on
+the host cores.  The product package fr_sdg_b200 never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_ref" / "libfrsdg_ref.so"
+
+_lib = None
+_P, _D = C.c_void_p, C.c_double
+
+
+def available() -> bool:
+    """The library is built (from the reference tree when it is present)."""
+    if LIB_PATH.exists():
+        return True
+    from oracle import ref_build
+
+    return ref_build.build() is not None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not available():
+            raise FileNotFoundError(f"{LIB_PATH} is not built and the reference tree is absent")
+        L = C.CDLL(str(LIB_PATH))
+        sig = {
+            "ref_last_error": (C.c_char_p, []),
+            "ref_create": (_P, [_P]),
+            "ref_destroy": (None, [_P]),
+            "ref_n_dofs": (C.c_int64, [_P]),
+            "ref_residual": (C.c_int, [_P, _D, _P, _P]),
+            "ref_residual_complex": (C.c_int, [_P, _D, _P, _P]),
+            "ref_rhs": (C.c_int, [_P, _D, _P, _P]),
+            "ref_ifunction": (C.c_int, [_P, _D, _P, _P, _P]),
+            "ref_jvp": (C.c_int, [_P, _D, _D, _P, _P, _P]),
+            "ref_post_step": (C.c_int, [_P, _P]),
+            "ref_prim_to_cons": (C.c_int, [_P, _P, _P]),
+            "ref_reference_element": (C.c_int, [C.c_int, _D, _P, _P, _P, _P, _P]),
+            "ref_filter_matrix": (C.c_int, [C.c_int, C.c_int, C.c_int, _D, _P]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray) -> int:
+    assert a.flags.c_contiguous
+    return a.ctypes.data
+
+
+def _chk(rc: int, what: str) -> None:
+    if rc != 0:
+        raise RuntimeError(f"{what}: {lib().ref_last_error().decode()}")
+
+
+class Reference:
+    """The reference's residual path for one configuration (single rank)."""
+
+    def __init__(self, cfg):
+        self._h = lib().ref_create(C.addressof(cfg))
+        if not self._h:
+            raise RuntimeError(lib().ref_last_error().decode())
+        self.n_dofs = int(lib().ref_n_dofs(self._h))
+
+    def close(self):
+        if self._h:
+            lib().ref_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _vec(self, a) -> np.ndarray:
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert a.size == self.n_dofs
+        return a
+
+    def residual(self, t: float, U) -> np.ndarray:
+        U = self._vec(U)
+        R = np.empty_like(U)
+        _chk(lib().ref_residual(self._h, t, _p(U), _p(R)), "ref_residual")
+        return R
+
+    def residual_complex(self, t: float, U) -> np.ndarray:
+        U = np.ascontiguousarray(U, dtype=np.complex128)
+        R = np.empty_like(U)
+        _chk(lib().ref_residual_complex(self._h, t, _p(U), _p(R)), "ref_residual_complex")
+        return R
+
+    def rhs(self, t: float, U) -> np.ndarray:
+        U = self._vec(U)
+        F = np.empty_like(U)
+        _chk(lib().ref_rhs(self._h, t, _p(U), _p(F)), "ref_rhs")
+        return F
+
+    def ifunction(self, t: float, U, Udot) -> np.ndarray:
+        U, Udot = self._vec(U), self._vec(Udot)
+        F = np.empty_like(U)
+        _chk(lib().ref_ifunction(self._h, t, _p(U), _p(Udot), _p(F)), "ref_ifunction")
+        return F
+
+    def jvp(self, t: float, sigma: float, U, V) -> np.ndarray:
+        U, V = self._vec(U), self._vec(V)
+        JV = np.empty_like(U)
+        _chk(lib().ref_jvp(self._h, t, sigma, _p(U), _p(V), _p(JV)), "ref_jvp")
+        return JV
+
+    def post_step(self, U) -> np.ndarray:
+        U = self._vec(U).copy()
+        _chk(lib().ref_post_step(self._h, _p(U)), "ref_post_step")
+        return U
+
+    def prim_to_cons(self, prim) -> np.ndarray:
+        prim = self._vec(prim)
+        out = np.empty_like(prim)
+        _chk(lib().ref_prim_to_cons(self._h, _p(prim), _p(out)), "ref_prim_to_cons")
+        return out
+
+
+def reference_element(p: int, c: float = 0.0):
+    n = p + 1
+    x, w, dl, dr = (np.zeros(n) for _ in range(4))
+    D = np.zeros((n, n))
+    _chk(lib().ref_reference_element(p, c, _p(x), _p(w), _p(D), _p(dl), _p(dr)), "ref_reference_element")
+    return x, w, D, dl, dr
+
+
+def filter_matrix(p: int, cut_off: int = 2, strength: int = 32, alpha: float = 36.0) -> np.ndarray:
+    n = p + 1
+    F = np.zeros((n, n))
+    _chk(lib().ref_filter_matrix(p, cut_off, strength, alpha, _p(F)), "ref_filter_matrix")
+    return F
