@@ -26,11 +26,16 @@ def make_config(dim: int = 2, p: int = 3, n_elems=(10, 10), box=(1.0, 1.0), rada
                 geometry: int = A.GEOM_CARTESIAN, profile: int = A.PROFILE_FLAT, geom_params=(0.0, 0.0, 0.0, 0.0),
                 bcs=None, apply_filter: bool = False, cut_off: int = 2, strength: int = 32, alpha: float = 36.0,
                 apply_weno: bool = False, weno_gamma: float = 0.998, theta: float = 1.0, threshold: float = 0.8,
-                cond_sys: bool = False, csd_eps: float = 1e-7, coord_sys: int = A.COORD_CARTESIAN) -> A.frsdg_config:
+                cond_sys: bool = False, csd_eps: float = 1e-7, coord_sys: int = A.COORD_CARTESIAN,
+                defaults: Callable[[A.frsdg_config], None] | None = None) -> A.frsdg_config:
     """Build a configuration; `bcs` maps a face (A.LEFT..A.BOTTOM) to a kind or
-    to (kind, state, params)."""
+    to (kind, state, params).  The remaining fields take the library's defaults
+    (frsdg_config_default), or those `defaults(cfg)` writes."""
     c = A.frsdg_config()
-    A.check(A.lib().frsdg_config_default(c), "frsdg_config_default")
+    if defaults is None:
+        A.check(A.lib().frsdg_config_default(c), "frsdg_config_default")
+    else:
+        defaults(c)
     c.dim, c.poly_deg = dim, p
     c.n_elems[0] = n_elems[0]
     c.n_elems[1] = n_elems[1] if dim == 2 else 1
@@ -62,13 +67,16 @@ def make_config(dim: int = 2, p: int = 3, n_elems=(10, 10), box=(1.0, 1.0), rada
 
 
 # ---------------------------------------------------------------- geometry on the host
-def node_coords(cfg: A.frsdg_config, device="cpu", rows: tuple[int, int] | None = None) -> tuple[torch.Tensor, torch.Tensor]:
+def node_coords(cfg: A.frsdg_config, device="cpu", rows: tuple[int, int] | None = None,
+                gll_nodes=None) -> tuple[torch.Tensor, torch.Tensor]:
     """Physical (x, y) of every node, shaped (Ny, Nx, n, n) [j, i, l, k] (2D) or
     (Nx, n) (1D).  Same analytic maps as the library's geometry policies.
     rows = (row_base, count): only `count` element rows from global row `row_base`
-    (rows outside [0, Ny) wrap around, as the ghost rows of a periodic partition)."""
+    (rows outside [0, Ny) wrap around, as the ghost rows of a periodic partition).
+    gll_nodes: the p + 1 GLL nodes to use (default: the library's reference element)."""
     p = cfg.poly_deg
-    x_ref = torch.tensor(reference_element(p)[0], dtype=torch.float64, device=device)
+    nodes = reference_element(p)[0] if gll_nodes is None else gll_nodes
+    x_ref = torch.tensor(nodes, dtype=torch.float64, device=device)
     if cfg.dim == 1:
         N = cfg.n_elems[0]
         h = cfg.box_length[0] / N
@@ -240,21 +248,24 @@ def bump_channel(nx: int = 256, ny: int = 64, p: int = 3, mach: float = 0.5) -> 
                     notes={"p_out": p_out})
 
 
-def blast_large(n_elems: int = 1024, p: int = 5, ny: int | None = None) -> Workload:
+def blast_large(n_elems: int = 1024, p: int = 5, ny: int | None = None, defaults=None,
+                gll_nodes=None) -> Workload:
     """2D radial blast on [0,1]^2, HLLC, Van der Waals (a=0.05, b=0.02, gamma=1.4),
     SSP-RK3, 200 steps, WENO + shock sensor (CFL 0.01: p = 5).  ny > n_elems stacks
     more rows of the same element size above it (box [0,1] x [0, ny/n_elems]): the
-    weak-scaling mesh of a row-block partition."""
+    weak-scaling mesh of a row-block partition.  `defaults` and `gll_nodes` replace
+    the library's configuration defaults and reference element (make_config,
+    node_coords), so that the same input can be built without the library."""
     a, b, g = 0.05, 0.02, 1.4
     ny = ny or n_elems
     cfg = make_config(dim=2, p=p, n_elems=(n_elems, ny), box=(1.0, ny / n_elems), riemann="hllc",
                       gas="vdw", gamma=g, vdw=(a, b),
                       bcs={A.LEFT: A.BC_OUTFLOW, A.RIGHT: A.BC_OUTFLOW, A.TOP: A.BC_OUTFLOW,
                            A.BOTTOM: A.BC_OUTFLOW},
-                      **SHOCK_STAB)
+                      defaults=defaults, **SHOCK_STAB)
 
     def init(device="cpu", rows=None):
-        x, y = node_coords(cfg, device, rows)
+        x, y = node_coords(cfg, device, rows, gll_nodes)
         r = torch.sqrt((x - 0.5) ** 2 + (y - 0.5) ** 2)
         inside = r < 0.4
         rho = torch.where(inside, 1.0, 0.125).to(torch.float64)

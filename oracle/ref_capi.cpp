@@ -28,7 +28,10 @@
 
 #include "../include/frsdg.h"
 
+#include <barrier>
 #include <complex>
+#include <exception>
+#include <thread>
 #include <cstring>
 #include <memory>
 #include <numbers>
@@ -271,29 +274,40 @@ struct RefProblem
     virtual void jvp(double t, double sigma, const double* U, const double* V, double* JV) = 0;
     virtual void post_step(double* U) = 0;
     virtual void prim_to_cons(const double* prim, double* cons) = 0;
+    virtual void set_threads(int) {}
+    // rhs_func: rhs = -R(U)
+    virtual void rhs(double t, const double* U, double* F)
+    {
+        residual(t, U, F);
+        const int64_t n = n_dofs();
+        for (int64_t q = 0; q < n; ++q) F[q] = -F[q];
+    }
     bool cond_sys{false};
 };
 
-// One-rank DMDA and the PETSc views on plain arrays.
+// One-rank DMDA and the vectors handed to the reference's PETSc views: global
+// vectors wrap the caller's arrays (no copy); local vectors come from the DM.
 struct Dmda
 {
     StubDM_ dm;
-    Vec make_global(const double* src)
-    {
-        auto* v = new StubVec_;
-        v->data.assign(src, src + size());
-        owned.emplace_back(v);
-        return v;
-    }
-    Vec make_global_zero()
-    {
-        auto* v = new StubVec_;
-        v->data.assign(size(), 0.0);
-        owned.emplace_back(v);
-        return v;
-    }
-    size_t size() const { return size_t(dm.nx) * (dm.dim == 2 ? dm.ny : 1) * dm.dof; }
     std::vector<std::unique_ptr<StubVec_>> owned;
+    size_t size() const { return size_t(dm.nx) * (dm.dim == 2 ? dm.ny : 1) * dm.dof; }
+    Vec wrap(const double* p)
+    {
+        owned.push_back(std::make_unique<StubVec_>());
+        owned.back()->ptr = const_cast<double*>(p);
+        owned.back()->n = size();
+        return owned.back().get();
+    }
+    Vec make_copy(const double* src)
+    {
+        owned.push_back(std::make_unique<StubVec_>());
+        StubVec_* v = owned.back().get();
+        v->own.assign(src, src + size());
+        v->ptr = v->own.data();
+        v->n = v->own.size();
+        return v;
+    }
     void release() { owned.clear(); }
 };
 
@@ -307,10 +321,15 @@ template <class Traits> struct RefProblemT<Traits, 2> final : RefProblem
     std::unique_ptr<PE>   phys;
     Dmda                  da;
 
+    BoundaryConditions<double, 2> bcs;
+    // host-thread form of the residual: one evaluator per thread, each owning a
+    // block of element rows (the DMDA ranges of one MPI rank of a 1 x T process grid)
+    std::vector<std::unique_ptr<PE>> parts;
+    std::vector<double> local_buf;  // the ghosted local vector of the threaded form
+
     explicit RefProblemT(const frsdg_config& c) : cfg(c), opts(make_options(c))
     {
         cond_sys = c.cond_sys != 0;
-        BoundaryConditions<double, 2> bcs;
         const Direction dirs[4] = {Direction::Left, Direction::Right, Direction::Top, Direction::Bottom};
         for (int f = 0; f < 4; ++f) bind(bcs, dirs[f], f);
         g_cfg = &cfg;
@@ -439,15 +458,87 @@ template <class Traits> struct RefProblemT<Traits, 2> final : RefProblem
 
     int64_t n_dofs() const override { return int64_t(da.size()); }
 
+    void set_threads(int n) override
+    {
+        parts.clear();
+        n = std::max(1, std::min(n, da.dm.ny));
+        if (n == 1) return;
+        for (int q = 0; q < n; ++q)
+        {
+            // contiguous row blocks, sizes differing by at most one (PETSC_DECIDE)
+            const int j0 = int(int64_t(da.dm.ny) * q / n), j1 = int(int64_t(da.dm.ny) * (q + 1) / n);
+            g_cfg = &cfg;
+            parts.push_back(std::make_unique<PE>(opts, bcs, typename Traits::GasModel{opts}));
+            g_cfg = nullptr;
+            DMInfos<2> inf = phys->m_dm_info;
+            inf.start[1] = j0;
+            inf.size[1] = j1 - j0;
+            inf.max[1] = j1;
+            parts.back()->m_dm_info = inf;
+        }
+    }
+
+    // rhs_func's residual with T host threads standing in for T MPI ranks: each
+    // scatters its own rows into the shared ghosted local vector (the rows of the
+    // mesh edges also their ghost row), waits for its neighbours, and runs
+    // residual_kernel over its rows, writing R directly.
+    void residual_threaded(double t, const double* U, double* R, bool negate = false)
+    {
+        const size_t nl = stub_local_size(&da.dm);
+        if (local_buf.size() != nl) local_buf.assign(nl, 0.0);
+        const int T = int(parts.size());
+        std::barrier sync(T);
+        std::vector<std::exception_ptr> failures(static_cast<size_t>(T));
+        std::exception_ptr* fail = failures.data();
+        std::vector<std::thread> th;
+        for (int q = 0; q < T; ++q)
+            th.emplace_back([&, q, fail] {
+                try
+                {
+                    PE& pe = *parts[size_t(q)];
+                    const int j0 = pe.m_dm_info.start[1], j1 = pe.m_dm_info.max[1];
+                    stub_scatter_rows(&da.dm, U, local_buf.data(), q == 0 ? -1 : j0, q == T - 1 ? j1 : j1 - 1);
+                    sync.arrive_and_wait();
+                    StubVec_ lv, gv;
+                    lv.ptr = local_buf.data();
+                    lv.n = nl;
+                    lv.local = true;
+                    gv.ptr = R;
+                    gv.n = da.size();
+                    ReadDOFView<2>  x{&da.dm, &lv, VecType::Global};  // already ghosted
+                    WriteDOFView<2> fv{&da.dm, &gv, VecType::Global};
+                    if (pe.template residual_kernel<double>(x, fv, t) != 0) throw std::runtime_error("residual_kernel");
+                    if (negate)  // VecScale(rhs, -1) of this rank's rows
+                    {
+                        const size_t row = size_t(da.dm.nx) * da.dm.dof;
+                        for (size_t q2 = size_t(j0) * row; q2 < size_t(j1) * row; ++q2) R[q2] = -R[q2];
+                    }
+                }
+                catch (...)
+                {
+                    fail[q] = std::current_exception();
+                }
+            });
+        for (auto& h : th) h.join();
+        for (auto& e : failures)
+            if (e) std::rethrow_exception(e);
+    }
+
+    void rhs(double t, const double* U, double* F) override
+    {
+        if (parts.size() > 1) return residual_threaded(t, U, F, true);
+        RefProblem::rhs(t, U, F);
+    }
+
     void residual(double t, const double* U, double* R) override
     {
-        Vec gu = da.make_global(U), gr = da.make_global_zero();
+        if (parts.size() > 1) return residual_threaded(t, U, R);
+        Vec gu = da.wrap(U), gr = da.wrap(R);
         {
             ReadDOFView<2>  x{&da.dm, gu, VecType::Local};
             WriteDOFView<2> fv{&da.dm, gr, VecType::Global};
             if (phys->template residual_kernel<double>(x, fv, t) != 0) throw std::runtime_error("residual_kernel");
         }
-        std::memcpy(R, gr->data.data(), sizeof(double) * da.size());
         da.release();
     }
 
@@ -466,12 +557,12 @@ template <class Traits> struct RefProblemT<Traits, 2> final : RefProblem
         {
             std::vector<double> tmp(da.size());
             for (size_t q = 0; q < tmp.size(); ++q) tmp[q] = part ? U[q].imag() : U[q].real();
-            g[part] = da.make_global(tmp.data());
+            g[part] = da.make_copy(tmp.data());
             DMGetLocalVector(&da.dm, &l[part]);
             DMGlobalToLocalEnd(&da.dm, g[part], INSERT_VALUES, l[part]);
         }
         std::vector<Cplx> u(n_ghosted()), f(n_ghosted());
-        for (size_t q = 0; q < u.size(); ++q) u[q] = Cplx(l[0]->data[q], l[1]->data[q]);
+        for (size_t q = 0; q < u.size(); ++q) u[q] = Cplx(l[0]->ptr[q], l[1]->ptr[q]);
         for (int part = 0; part < 2; ++part) DMRestoreLocalVector(&da.dm, &l[part]);
         ReadCplxView<2>  uv{u, phys->m_dm_info};
         WriteCplxView<2> fv{f, phys->m_dm_info};
@@ -495,7 +586,7 @@ template <class Traits> struct RefProblemT<Traits, 2> final : RefProblem
         const double h = cfg.csd_eps, one_over_h = 1.0 / h;
         const auto& dminfo = phys->m_dm_info;
         std::vector<Cplx> u_pl_iv(n_ghosted()), jv_buff(n_ghosted());
-        Vec gu = da.make_global(U), gv = da.make_global(V), gjv = da.make_global_zero();
+        Vec gu = da.wrap(U), gv = da.wrap(V), gjv = da.wrap(JV);
         {
             WriteCplxView<2> u_iv_view{u_pl_iv, dminfo};
             ReadDOFView<2>   v_view{&da.dm, gv, VecType::Local};
@@ -546,32 +637,29 @@ template <class Traits> struct RefProblemT<Traits, 2> final : RefProblem
                     for (size_t q = 0; q < jv_sp.size(); ++q) jv_sp[q] += std::imag(f_sp[q]) * one_over_h;
                 }
         }
-        std::memcpy(JV, gjv->data.data(), sizeof(double) * da.size());
         da.release();
     }
 
     // apply_stabilization (petsc_solver_impl.hpp:683-702): limit a copy into the state
     void post_step(double* U) override
     {
-        Vec filtered = da.make_global(U), sol = da.make_global(U);
+        Vec filtered = da.make_copy(U), sol = da.wrap(U);  // VecCopy(solution, u_filtered)
         {
             ReadDOFView<2>  s{&da.dm, filtered, VecType::Local};
             WriteDOFView<2> o{&da.dm, sol, VecType::Global};
             if (phys->template limit_solution<double>(s, o) != 0) throw std::runtime_error("limit_solution");
         }
-        std::memcpy(U, sol->data.data(), sizeof(double) * da.size());
         da.release();
     }
 
     void prim_to_cons(const double* prim, double* cons) override
     {
-        Vec in = da.make_global(prim), out = da.make_global_zero();
+        Vec in = da.wrap(prim), out = da.wrap(cons);
         {
             ReadDOFView<2>  iv{&da.dm, in, VecType::Global};
             WriteDOFView<2> ov{&da.dm, out, VecType::Global};
             if (phys->template prim_to_cons_kernel<double>(iv, ov) != 0) throw std::runtime_error("prim_to_cons");
         }
-        std::memcpy(cons, out->data.data(), sizeof(double) * da.size());
         da.release();
     }
 };
@@ -612,13 +700,12 @@ template <class Traits> struct RefProblemT<Traits, 1> final : RefProblem
 
     void residual(double t, const double* U, double* R) override
     {
-        Vec gu = da.make_global(U), gr = da.make_global_zero();
+        Vec gu = da.wrap(U), gr = da.wrap(R);
         {
             ReadDOFView<1>  x{&da.dm, gu, VecType::Local};
             WriteDOFView<1> fv{&da.dm, gr, VecType::Global};
             if (phys->template residual_kernel<double>(x, fv, t) != 0) throw std::runtime_error("residual_kernel");
         }
-        std::memcpy(R, gr->data.data(), sizeof(double) * da.size());
         da.release();
     }
 
@@ -631,12 +718,12 @@ template <class Traits> struct RefProblemT<Traits, 1> final : RefProblem
         {
             std::vector<double> tmp(da.size());
             for (size_t q = 0; q < tmp.size(); ++q) tmp[q] = part ? U[q].imag() : U[q].real();
-            g[part] = da.make_global(tmp.data());
+            g[part] = da.make_copy(tmp.data());
             DMGetLocalVector(&da.dm, &l[part]);
             DMGlobalToLocalEnd(&da.dm, g[part], INSERT_VALUES, l[part]);
         }
         std::vector<Cplx> u(n_ghosted()), f(n_ghosted());
-        for (size_t q = 0; q < u.size(); ++q) u[q] = Cplx(l[0]->data[q], l[1]->data[q]);
+        for (size_t q = 0; q < u.size(); ++q) u[q] = Cplx(l[0]->ptr[q], l[1]->ptr[q]);
         for (int part = 0; part < 2; ++part) DMRestoreLocalVector(&da.dm, &l[part]);
         ReadCplxView<1>  uv{u, phys->m_dm_info};
         WriteCplxView<1> fv{f, phys->m_dm_info};
@@ -658,7 +745,7 @@ template <class Traits> struct RefProblemT<Traits, 1> final : RefProblem
         const double h = cfg.csd_eps, one_over_h = 1.0 / h;
         const auto& dminfo = phys->m_dm_info;
         std::vector<Cplx> u_pl_iv(n_ghosted()), jv_buff(n_ghosted());
-        Vec gu = da.make_global(U), gv = da.make_global(V), gjv = da.make_global_zero();
+        Vec gu = da.wrap(U), gv = da.wrap(V), gjv = da.wrap(JV);
         {
             WriteCplxView<1> u_iv_view{u_pl_iv, dminfo};
             ReadDOFView<1>   v_view{&da.dm, gv, VecType::Local};
@@ -701,31 +788,28 @@ template <class Traits> struct RefProblemT<Traits, 1> final : RefProblem
                 for (size_t q = 0; q < jv_sp.size(); ++q) jv_sp[q] += std::imag(f_sp[q]) * one_over_h;
             }
         }
-        std::memcpy(JV, gjv->data.data(), sizeof(double) * da.size());
         da.release();
     }
 
     void post_step(double* U) override
     {
-        Vec filtered = da.make_global(U), sol = da.make_global(U);
+        Vec filtered = da.make_copy(U), sol = da.wrap(U);  // VecCopy(solution, u_filtered)
         {
             ReadDOFView<1>  s{&da.dm, filtered, VecType::Local};
             WriteDOFView<1> o{&da.dm, sol, VecType::Global};
             if (phys->template limit_solution<double>(s, o) != 0) throw std::runtime_error("limit_solution");
         }
-        std::memcpy(U, sol->data.data(), sizeof(double) * da.size());
         da.release();
     }
 
     void prim_to_cons(const double* prim, double* cons) override
     {
-        Vec in = da.make_global(prim), out = da.make_global_zero();
+        Vec in = da.wrap(prim), out = da.wrap(cons);
         {
             ReadDOFView<1>  iv{&da.dm, in, VecType::Global};
             WriteDOFView<1> ov{&da.dm, out, VecType::Global};
             if (phys->template prim_to_cons_kernel<double>(iv, ov) != 0) throw std::runtime_error("prim_to_cons");
         }
-        std::memcpy(cons, out->data.data(), sizeof(double) * da.size());
         da.release();
     }
 };
@@ -802,6 +886,9 @@ void* ref_create(const frsdg_config* cfg)
 
 void ref_destroy(void* h) { delete static_cast<RefProblem*>(h); }
 
+// Residuals of 2D problems on n host threads (row blocks; see residual_threaded).
+void ref_set_threads(void* h, int n) { static_cast<RefProblem*>(h)->set_threads(n); }
+
 int64_t ref_n_dofs(void* h) { return static_cast<RefProblem*>(h)->n_dofs(); }
 
 int ref_residual(void* h, double t, const double* U, double* R)
@@ -819,12 +906,7 @@ int ref_residual_complex(void* h, double t, const double* U, double* R)
 // rhs_func: rhs = -R(U)
 int ref_rhs(void* h, double t, const double* U, double* F)
 {
-    return guarded([&] {
-        auto* P = static_cast<RefProblem*>(h);
-        P->residual(t, U, F);
-        const int64_t n = P->n_dofs();
-        for (int64_t q = 0; q < n; ++q) F[q] = -F[q];
-    });
+    return guarded([&] { static_cast<RefProblem*>(h)->rhs(t, U, F); });
 }
 
 // fun_implicit: F = U_t + R(M(U)), M = prim->cons on the owned elements when cond_sys

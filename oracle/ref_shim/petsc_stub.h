@@ -116,15 +116,22 @@ struct StubDM_
     int dim{2};
     int nx{1}, ny{1}, dof{1};
     bool per_x{false}, per_y{false};
-    std::vector<StubVec_*> pool;  // local vectors handed out by DMGetLocalVector
+    // local vectors handed out by DMGetLocalVector and kept for reuse, like PETSc's
+    // pool (a reused vector keeps its ghost entries, which nothing writes at a
+    // ghosted boundary, so they stay zero)
+    std::vector<std::pair<StubVec_*, bool>> pool;
     ~StubDM_();
 };
 typedef StubDM_* DM;
 
+// A vector is a view of `n` doubles at `ptr`: storage it owns (the DM's local
+// vectors) or memory of the caller (global vectors wrap the caller's arrays).
 struct StubVec_
 {
-    std::vector<double> data;
-    bool local{false};
+    std::vector<double> own;
+    double* ptr{nullptr};
+    size_t  n{0};
+    bool    local{false};
     // pointer tables handed out by DMDAVecGetArrayDOF(Read)
     std::vector<double*>  rows1;
     std::vector<double**> rows2;
@@ -133,12 +140,13 @@ typedef StubVec_* Vec;
 
 inline StubDM_::~StubDM_()
 {
-    for (auto* v : pool) delete v;
+    for (auto& v : pool) delete v.first;
 }
 
 // Element ranges: owned [0, n), ghosted [-1, n+1) along every axis (stencil width 1).
 inline int stub_ghost_w(const StubDM_* d) { return d->nx + 2; }
 inline int stub_ghost_h(const StubDM_* d) { return d->dim == 2 ? d->ny + 2 : 1; }
+inline size_t stub_local_size(const StubDM_* d) { return size_t(stub_ghost_w(d)) * stub_ghost_h(d) * d->dof; }
 
 inline PetscErrorCode DMDAGetCorners(DM da, PetscInt* x, PetscInt* y, PetscInt* z, PetscInt* m, PetscInt* n,
                                      PetscInt* p)
@@ -165,22 +173,26 @@ inline PetscErrorCode DMDAGetGhostCorners(DM da, PetscInt* x, PetscInt* y, Petsc
 
 inline PetscErrorCode DMGetLocalVector(DM da, Vec* v)
 {
+    for (auto& e : da->pool)
+        if (!e.second)
+        {
+            e.second = true;
+            *v = e.first;
+            return 0;
+        }
     auto* lv  = new StubVec_;
     lv->local = true;
-    lv->data.assign(size_t(stub_ghost_w(da)) * stub_ghost_h(da) * da->dof, 0.0);
-    da->pool.push_back(lv);
+    lv->own.assign(stub_local_size(da), 0.0);
+    lv->ptr = lv->own.data();
+    lv->n   = lv->own.size();
+    da->pool.emplace_back(lv, true);
     *v = lv;
     return 0;
 }
 inline PetscErrorCode DMRestoreLocalVector(DM da, Vec* v)
 {
-    for (size_t q = 0; q < da->pool.size(); ++q)
-        if (da->pool[q] == *v)
-        {
-            delete da->pool[q];
-            da->pool.erase(da->pool.begin() + static_cast<std::ptrdiff_t>(q));
-            break;
-        }
+    for (auto& e : da->pool)
+        if (e.first == *v) e.second = false;
     *v = nullptr;
     return 0;
 }
@@ -192,11 +204,12 @@ inline size_t stub_local_off(const StubDM_* d, int i, int j)
     return (size_t(jj) * stub_ghost_w(d) + size_t(i + 1)) * d->dof;
 }
 
-inline PetscErrorCode DMGlobalToLocalBegin(DM, Vec, InsertMode, Vec) { return 0; }
-inline PetscErrorCode DMGlobalToLocalEnd(DM da, Vec g, InsertMode, Vec l)
+// The ghost scatter of rows [j_lo, j_hi] (inclusive; 2D rows may reach -1 and ny,
+// 1D uses row 0) from the global array g into the local array l: owned elements
+// and the periodic wrap; ghosts at a ghosted boundary are left as they are.
+inline void stub_scatter_rows(const StubDM_* da, const double* g, double* l, int j_lo, int j_hi)
 {
-    const int jlo = da->dim == 2 ? -1 : 0, jhi = da->dim == 2 ? da->ny : 0;
-    for (int j = jlo; j <= jhi; ++j)
+    for (int j = j_lo; j <= j_hi; ++j)
         for (int i = -1; i <= da->nx; ++i)
         {
             int si = i, sj = j;
@@ -211,10 +224,17 @@ inline PetscErrorCode DMGlobalToLocalEnd(DM da, Vec g, InsertMode, Vec l)
                 if (!da->per_y) ok = false;
                 sj = (sj + da->ny) % da->ny;
             }
-            if (!ok) continue;  // ghosted (non-periodic) boundary: left as it is (zero)
+            if (!ok) continue;
             const size_t go = (size_t(da->dim == 2 ? sj : 0) * da->nx + size_t(si)) * da->dof;
-            std::memcpy(l->data.data() + stub_local_off(da, i, j), g->data.data() + go, sizeof(double) * da->dof);
+            std::memcpy(l + stub_local_off(da, i, j), g + go, sizeof(double) * da->dof);
         }
+}
+
+inline PetscErrorCode DMGlobalToLocalBegin(DM, Vec, InsertMode, Vec) { return 0; }
+inline PetscErrorCode DMGlobalToLocalEnd(DM da, Vec g, InsertMode, Vec l)
+{
+    if (da->dim == 2) stub_scatter_rows(da, g->ptr, l->ptr, -1, da->ny);
+    else stub_scatter_rows(da, g->ptr, l->ptr, 0, 0);
     return 0;
 }
 
@@ -224,7 +244,7 @@ inline PetscErrorCode DMDAVecGetArrayDOF(DM da, Vec v, void* arr)
     {
         const int lo = v->local ? -1 : 0, cnt = v->local ? da->nx + 2 : da->nx;
         v->rows1.assign(size_t(cnt), nullptr);
-        for (int i = 0; i < cnt; ++i) v->rows1[size_t(i)] = v->data.data() + size_t(i) * da->dof;
+        for (int i = 0; i < cnt; ++i) v->rows1[size_t(i)] = v->ptr + size_t(i) * da->dof;
         *static_cast<double***>(arr) = v->rows1.data() - lo;
         return 0;
     }
@@ -234,8 +254,7 @@ inline PetscErrorCode DMDAVecGetArrayDOF(DM da, Vec v, void* arr)
     v->rows2.assign(size_t(h), nullptr);
     for (int j = 0; j < h; ++j)
     {
-        for (int i = 0; i < w; ++i)
-            v->rows1[size_t(j) * w + i] = v->data.data() + (size_t(j) * w + i) * da->dof;
+        for (int i = 0; i < w; ++i) v->rows1[size_t(j) * w + i] = v->ptr + (size_t(j) * w + i) * da->dof;
         v->rows2[size_t(j)] = v->rows1.data() + size_t(j) * w - lo;
     }
     *static_cast<double****>(arr) = v->rows2.data() - lo;

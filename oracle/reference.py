@@ -41,6 +41,7 @@ def lib() -> C.CDLL:
             "ref_create": (_P, [_P]),
             "ref_destroy": (None, [_P]),
             "ref_n_dofs": (C.c_int64, [_P]),
+            "ref_set_threads": (None, [_P, C.c_int]),
             "ref_residual": (C.c_int, [_P, _D, _P, _P]),
             "ref_residual_complex": (C.c_int, [_P, _D, _P, _P]),
             "ref_rhs": (C.c_int, [_P, _D, _P, _P]),
@@ -72,11 +73,19 @@ def _chk(rc: int, what: str) -> None:
 class Reference:
     """The reference's residual path for one configuration (single rank)."""
 
-    def __init__(self, cfg):
+    def __init__(self, cfg, threads: int = 1):
         self._h = lib().ref_create(C.addressof(cfg))
         if not self._h:
             raise RuntimeError(lib().ref_last_error().decode())
         self.n_dofs = int(lib().ref_n_dofs(self._h))
+        if threads > 1:
+            self.set_threads(threads)
+
+    def set_threads(self, n: int) -> None:
+        """2D residuals on n host threads, each owning a block of element rows as one
+        MPI rank of the reference would (the ghost scatter and the residual of the
+        block run on that thread)."""
+        lib().ref_set_threads(self._h, n)
 
     def close(self):
         if self._h:
@@ -106,9 +115,9 @@ class Reference:
         _chk(lib().ref_residual_complex(self._h, t, _p(U), _p(R)), "ref_residual_complex")
         return R
 
-    def rhs(self, t: float, U) -> np.ndarray:
+    def rhs(self, t: float, U, out: np.ndarray | None = None) -> np.ndarray:
         U = self._vec(U)
-        F = np.empty_like(U)
+        F = np.empty_like(U) if out is None else out
         _chk(lib().ref_rhs(self._h, t, _p(U), _p(F)), "ref_rhs")
         return F
 
@@ -134,6 +143,29 @@ class Reference:
         out = np.empty_like(prim)
         _chk(lib().ref_prim_to_cons(self._h, _p(prim), _p(out)), "ref_prim_to_cons")
         return out
+
+
+def default_config(c) -> None:
+    """Fill a frsdg_config with the reference's defaults without the CUDA library:
+    Parser::parse_options (parser.hpp:257-300: 10 elements, p = 3, box 1, c = 0),
+    ConfigOptions and its option structs (parser.hpp:45-91: filter cut-off 2,
+    strength 32, alpha 36, WENO gamma 0.998, shock theta 1, threshold 0.8, ideal gas
+    gamma 1.4, R 287.05, VdW a 161.94, b 0.001265), outflow faces
+    (boundary_conditions.hpp:229-235) and the complex step 1e-7
+    (petsc_solver_impl.hpp:179)."""
+    C.memset(C.addressof(c), 0, C.sizeof(c))
+    c.dim, c.poly_deg = 2, 3
+    c.n_elems[0] = c.n_elems[1] = 10
+    c.box_length[0] = c.box_length[1] = 1.0
+    c.radau_corr = 0.0
+    c.gas_law, c.riemann = 0, 0
+    c.gamma, c.R_spec, c.vdw_a, c.vdw_b = 1.4, 287.05, 161.94, 0.001265
+    c.coord_sys = c.geometry = c.geom_profile = 0
+    for f in range(4):
+        c.bc[f].kind = 0
+    c.apply_filter, c.filt_cut_off, c.filt_strength, c.filt_alpha = 0, 2, 32, 36.0
+    c.apply_weno, c.weno_gamma, c.shock_theta, c.shock_threshold = 0, 0.998, 1.0, 0.8
+    c.cond_sys, c.jvp_exact_bc, c.csd_eps = 0, 0, 1e-7
 
 
 def reference_element(p: int, c: float = 0.0):

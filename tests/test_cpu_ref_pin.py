@@ -160,3 +160,32 @@ def test_oracle_vs_reference_1d(name):
     Us = random_state(cfg, seed=43, smooth=True)
     P = cons_to_prim(cfg, Us)
     assert rel_err(O.Oracle(cfg).prim_to_cons(P), ref.Reference(cfg).prim_to_cons(P)) <= TOL_FP64
+
+
+@pytest.mark.parametrize("threads", [2, 3, 5])
+def test_reference_threaded_rhs_is_the_single_thread_rhs(threads):
+    """The reference arm's host-thread form (one block of element rows per thread, as
+    MPI ranks) computes the same numbers as the one-rank residual."""
+    ref = _reference()
+    for name in ("cart_vdw_rusanov_p5_perx", "vortex_dirichlet_p3", "bump_hllc_p3_inflow_outlet"):
+        cfg = _cfg2d(**CASES_2D[name])
+        U = random_state(cfg, seed=3)
+        one = ref.Reference(cfg).rhs(0.1, U)
+        many = ref.Reference(cfg, threads=threads).rhs(0.1, U)
+        assert np.array_equal(one, many), name
+        assert np.array_equal(ref.Reference(cfg, threads=threads).residual(0.1, U), -one), name
+
+
+def test_reference_default_config_is_the_library_default():
+    """The reference arm builds its configuration without the CUDA library; its
+    defaults equal frsdg_config_default field by field."""
+    import ctypes
+
+    from fr_sdg_b200 import _abi as A
+    from oracle import reference
+
+    a, b = A.frsdg_config(), A.frsdg_config()
+    A.check(A.lib().frsdg_config_default(a), "frsdg_config_default")
+    reference.default_config(b)
+    assert ctypes.string_at(ctypes.addressof(a), ctypes.sizeof(a)) == ctypes.string_at(ctypes.addressof(b),
+                                                                                           ctypes.sizeof(b))
