@@ -221,6 +221,19 @@ def cpu_residual_rate(threads: int, target_s: float = 3.0, rows: int = 64, max_r
                               "cores": threads}
 
 
+def repo_libraries_loaded() -> list[str]:
+    """Shared libraries of this repository mapped into the process (Linux)."""
+    out = set()
+    try:
+        for line in Path("/proc/self/maps").read_text().splitlines():
+            path = line.split()[-1] if line.strip() else ""
+            if path.endswith(".so") and path.startswith(str(ROOT)):
+                out.add(str(Path(path).relative_to(ROOT)))
+    except OSError:
+        pass
+    return sorted(out)
+
+
 def reference_input(elements: int):
     """The workload's configuration and initial state built without libfrsdg.so:
     the reference's defaults (oracle/reference.py::default_config) and the GLL
@@ -272,6 +285,7 @@ def run_reference(args, ws, rank):
                                    "oracle/_ref/libfrsdg_ref.so against stand-ins for PETSc/Eigen/Boost; "
                                    f"median step {statistics.median(step_s) * 1e3:.0f} ms"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "libraries_loaded": repo_libraries_loaded(),
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -1,5 +1,5 @@
-"""The benchmark contract: bench.py's reference arm (CPU: the oracle restatement on the
-host cores) and our arm (GPU, on a 64^2 version of the workload) each print one JSON
+"""The benchmark contract: bench.py's reference arm (CPU: fr_sdg's own residual code,
+oracle/_ref, on the host cores) and our arm (GPU, on a 64^2 version of the workload) each print one JSON
 line with the keys of the contract."""
 from __future__ import annotations
 
@@ -25,8 +25,11 @@ def test_reference_arm_line():
         assert key in d, key
     assert d["impl"] == "reference" and d["value"] > 0 and d["steps"] == 2 and d["warmup"] == 1
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
-    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
     assert d["config"]["workload"].startswith("blast_vdw_1024x1024_p5")
+    assert d["config"]["elements"] == [1024, 1024] and d["ms_per_step"] > 0
+    # the reference arm runs the reference's code alone: the CUDA library is never loaded
+    assert d["libraries_loaded"] == ["oracle/_ref/libfrsdg_ref.so"]
 
 
 @pytest.mark.gpu
