@@ -508,7 +508,7 @@ def run_ours(args, ws, rank, local):
             torch.cuda.synchronize()
             del _g, _warm
             U1 = wl.init(f"cuda:{local}")
-            dt = cfl_time_step(wl.cfg, U1, wl.cfl)
+            dt = wl.time_step(U1)
             integ = Integrator(solver, "ssprk3")
             integ.step(U1, 0.0, dt)  # warm (allocates the stage buffers)
             U1.copy_(wl.init(f"cuda:{local}"))
@@ -521,7 +521,7 @@ def run_ours(args, ws, rank, local):
             vw = vortex_curved()
             with FRSolver(vw.cfg) as vs:
                 V = vw.init(f"cuda:{local}")
-                vdt = cfl_time_step(vw.cfg, V, vw.cfl)
+                vdt = vw.time_step(V)
                 vint = Integrator(vs, "rk4")
                 vint.step(V, 0.0, vdt)
                 V.copy_(vw.init(f"cuda:{local}"))
@@ -540,7 +540,7 @@ def run_ours(args, ws, rank, local):
             sw = sod1d()
             with FRSolver(sw.cfg) as ss:
                 S = sw.init(f"cuda:{local}")
-                sdt = cfl_time_step(sw.cfg, S, sw.cfl)
+                sdt = sw.time_step(S)
                 sint = Integrator(ss, "ssprk3")
                 sint.step(S, 0.0, sdt)
                 S.copy_(sw.init(f"cuda:{local}"))

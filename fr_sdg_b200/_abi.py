@@ -47,6 +47,7 @@ class frsdg_config(C.Structure):
         ("shock_theta", C.c_double), ("shock_threshold", C.c_double),
         ("cond_sys", C.c_int32), ("jvp_exact_bc", C.c_int32),
         ("csd_eps", C.c_double),
+        ("pp_limit", C.c_int32), ("pad1_", C.c_int32), ("pp_eps", C.c_double),
     ]
 
 
@@ -78,6 +79,7 @@ SIGNATURES = {
     "frsdg_post_step_to": (C.c_int, [_P, _P, _P, _P]),
     "frsdg_post_step_static": (C.c_int, [C.POINTER(frsdg_config), _P, _P]),
     "frsdg_prim_to_cons": (C.c_int, [_P, _P, _P, _P]),
+    "frsdg_pp_limit": (C.c_int, [_P, _P, _P, _P]),
     "frsdg_rhs_host": (C.c_int, [_P, _D, _P, _P, _P]),
     "frsdg_status": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "frsdg_petsc_vec_record_bytes": (C.c_int, [C.c_int64, C.c_int32, C.POINTER(C.c_int64)]),

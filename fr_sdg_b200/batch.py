@@ -120,7 +120,7 @@ class BatchedInstances:
             s.close()
         self.items = []
 
-    def run(self, t_end: float | None, cfl: float, graph: bool = True, n_steps: int | None = None,
+    def run(self, t_end: float | None, cfl: float | None = None, graph: bool = True, n_steps: int | None = None,
             steps_per_graph: int = 64) -> BatchResult:
         """Advance every instance to t_end (or by n_steps steps) with its own CFL time
         step; device-timed from the first launch to the last completion over all
@@ -132,7 +132,7 @@ class BatchedInstances:
         e1 = torch.cuda.Event(enable_timing=True)
         for _, s, _, _ in self.items:
             s.status()
-        dts = [cfl_time_step(wl.cfg, U, cfl) for wl, _, U, _ in self.items]
+        dts = [cfl_time_step(wl.cfg, U, wl.cfl if cfl is None else cfl, wl.cfl_rule) for wl, _, U, _ in self.items]
         graphs, t_cap = None, 0.0
         if graph and t_end is None and n_steps is not None and n_steps >= steps_per_graph:
             c0 = time.perf_counter()

@@ -9,6 +9,7 @@
 #include "frsdg_internal.hpp"
 #include "setup_ops.hpp"
 #include "jacobi.hpp"
+#include "pplimit.hpp"
 #include "stab.hpp"
 
 #include <algorithm>
@@ -121,6 +122,7 @@ int validate_config(const frsdg_config& c)
         return fail(FRSDG_ERR_ARG, "filter cut-off equal to poly_deg gives 0/0 in the filter strength");
     if (c.apply_weno && (c.weno_gamma > 1.0 || c.weno_gamma < 0.0)) return fail(FRSDG_ERR_ARG, "weno_gamma must be in [0,1]");
     if (!(c.csd_eps > 0.0)) return fail(FRSDG_ERR_ARG, "csd_eps must be positive");
+    if (c.pp_limit && !(c.pp_eps > 0.0)) return fail(FRSDG_ERR_ARG, "pp_eps must be positive");
     return FRSDG_OK;
 }
 
@@ -142,6 +144,8 @@ struct frsdg_handle
     double*      d_xnorm = nullptr;
     double*      d_ynorm = nullptr;
     double*      d_bxy = nullptr;
+    double*      d_detJ = nullptr;   // positivity limiter on curved meshes: detJ per node
+    PPArgs       pp{};               // template of the positivity limiter's launch
     double*      d_work = nullptr;   // post-step source copy (WENO)
     double*      d_stage = nullptr;  // host-buffer staging (2 * ntot), allocated on first use
     unsigned long long* d_bad = nullptr;
@@ -187,6 +191,7 @@ static void free_handle(frsdg_handle* h)
     cudaFree(h->d_xnorm);
     cudaFree(h->d_ynorm);
     cudaFree(h->d_bxy);
+    cudaFree(h->d_detJ);
     cudaFree(h->d_work);
     cudaFree(h->d_stage);
     cudaFree(h->d_bad);
@@ -248,6 +253,8 @@ int frsdg_config_default(frsdg_config* c)
     c->shock_threshold = 0.8;
     c->cond_sys = 0;
     c->csd_eps = 1e-7;
+    c->pp_limit = 0;
+    c->pp_eps = 1e-13;
     return FRSDG_OK;
 }
 
@@ -417,6 +424,28 @@ int frsdg_create(const frsdg_config* cfg, frsdg_handle** out)
                     free_handle(h);
                     return rc;
                 }
+                if (cfg->pp_limit)
+                {
+                    // detJ of the composite map at every node: the positivity limiter's
+                    // quadrature weights (physics_evaluator.hpp:282-305)
+                    std::vector<double> dj(size_t(h->nelem) * n * n);
+                    for (int j = 0; j < Ny; ++j)
+                        for (int i = 0; i < Nx; ++i)
+                            for (int l = 0; l < n; ++l)
+                                for (int k = 0; k < n; ++k)
+                                {
+                                    const GeomJacobian g = geom.jacobian(comp_x(i, k), comp_y(j, l));
+                                    const double dcsi_dr = 0.5 / double(Nx), deta_ds = 0.5 / double(Ny);
+                                    dj[((size_t(j) * Nx + i) * n + l) * n + k] =
+                                        (g.dx_dcsi * dcsi_dr) * (g.dy_deta * deta_ds) -
+                                        (g.dx_deta * deta_ds) * (g.dy_dcsi * dcsi_dr);
+                                }
+                    if ((rc = upload(&h->d_detJ, dj)))
+                    {
+                        free_handle(h);
+                        return rc;
+                    }
+                }
             }
             // boundary face points: LEFT, RIGHT (Ny*n each), TOP, BOTTOM (Nx*n each)
             std::vector<double> bxy(size_t(2 * Ny * n + 2 * Nx * n) * 2);
@@ -477,6 +506,21 @@ int frsdg_create(const frsdg_config* cfg, frsdg_handle** out)
         }
         a.ops = ops;
         a.bad = h->d_bad;
+    }
+
+    // positivity limiter
+    {
+        PPArgs& p = h->pp;
+        p.dim = cfg->dim;
+        p.n = n;
+        p.gas_law = cfg->gas_law;
+        p.gas = gas;
+        p.eps0 = cfg->pp_eps;
+        p.Nx = h->Nx;
+        p.Ny = h->Ny;
+        p.row_base = 0;
+        for (int q = 0; q < n; ++q) p.w[q] = h->re.w[q];
+        p.detJ = h->d_detJ;
     }
 
     // post-step stabilisation
@@ -836,12 +880,41 @@ int frsdg_pc_apply(frsdg_handle* h, const double* r, double* z, void* stream)
     return FRSDG_OK;
 }
 
+// The positivity limiter over the handle's vectors (whole mesh or row window).
+static int run_pp_limit(frsdg_handle* h, double* U, float* U32, cudaStream_t s)
+{
+    if (!h->cfg.pp_limit) return FRSDG_OK;
+    PPArgs p = h->pp;
+    p.U = U;
+    p.U32 = U32;
+    p.nelem = local_nelem(h);
+    p.row_base = h->win_rows ? h->win_base : 0;
+    const cudaError_t e = launch_pp_limit(p, s);
+    if (e != cudaSuccess) return cuda_fail(e, "positivity-limiter launch");
+    return FRSDG_OK;
+}
+
+int frsdg_pp_limit(frsdg_handle* h, double* U, float* U32, void* stream)
+{
+    if (!h || !U) return fail(FRSDG_ERR_ARG, "null argument");
+    if ((reinterpret_cast<uintptr_t>(U) | reinterpret_cast<uintptr_t>(U32)) & 15)
+        return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
+    if (U32 && h->cfg.dim != 2) return fail(FRSDG_ERR_ARG, "frsdg_pp_limit: the FP32 copy is 2D only");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    h->last = s;
+    return run_pp_limit(h, U, U32, s);
+}
+
 int frsdg_post_step(frsdg_handle* h, double* U, void* stream)
 {
     if (!h || !U) return fail(FRSDG_ERR_ARG, "null argument");
     if (reinterpret_cast<uintptr_t>(U) & 15) return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
-    if (!h->cfg.apply_filter && !h->cfg.apply_weno) return FRSDG_OK;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!h->cfg.apply_filter && !h->cfg.apply_weno)
+    {
+        h->last = s;
+        return run_pp_limit(h, U, nullptr, s);
+    }
     h->last = s;
     StabArgs a = h->st;
     a.dst = U;
@@ -859,7 +932,7 @@ int frsdg_post_step(frsdg_handle* h, double* U, void* stream)
     }
     cudaError_t e = launch_stab(h->n, a, s);
     if (e != cudaSuccess) return cuda_fail(e, "post-step launch");
-    return FRSDG_OK;
+    return run_pp_limit(h, U, nullptr, s);
 }
 
 int frsdg_post_step_to(frsdg_handle* h, const double* src, double* dst, void* stream)
@@ -874,7 +947,7 @@ int frsdg_post_step_to(frsdg_handle* h, const double* src, double* dst, void* st
     {
         cudaError_t e = cudaMemcpyAsync(dst, src, sizeof(double) * local_ntot(h), cudaMemcpyDeviceToDevice, s);
         if (e != cudaSuccess) return cuda_fail(e, "post-step copy");
-        return FRSDG_OK;
+        return run_pp_limit(h, dst, nullptr, s);
     }
     StabArgs a = h->st;
     a.src = src;
@@ -886,7 +959,7 @@ int frsdg_post_step_to(frsdg_handle* h, const double* src, double* dst, void* st
     }
     cudaError_t e = launch_stab(h->n, a, s);
     if (e != cudaSuccess) return cuda_fail(e, "post-step launch");
-    return FRSDG_OK;
+    return run_pp_limit(h, dst, nullptr, s);
 }
 
 int frsdg_prim_to_cons(frsdg_handle* h, const double* prim, double* cons, void* stream)

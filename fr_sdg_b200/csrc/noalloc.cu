@@ -62,6 +62,8 @@ extern "C" int frsdg_post_step_static(const frsdg_config* cfg, double* U, void* 
     if (reinterpret_cast<uintptr_t>(U) & 15) return report(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
     int rc = validate_config(*cfg);
     if (rc) return rc;
+    if (cfg->pp_limit)
+        return report(FRSDG_ERR_UNSUPPORTED, "frsdg_post_step_static: the positivity limiter needs a handle");
     const int n = cfg->poly_deg + 1;
     const int Nx = cfg->n_elems[0], Ny = cfg->dim == 2 ? cfg->n_elems[1] : 1;
     const int64_t ntot = int64_t(Nx) * Ny * (cfg->dim == 2 ? 4 * n * n : 3 * n);

@@ -1,0 +1,216 @@
+// pplimit.cu -- positivity-preserving scaling limiter (Zhang and Shu, "On
+// positivity-preserving high order discontinuous Galerkin schemes for compressible
+// Euler equations on rectangular meshes", J. Comput. Phys. 229 (2010) 8918-8934,
+// sec. 3), per element, in place:
+//   Ubar = GLL-quadrature cell average (weights w_k w_l detJ_kl in 2D, w_k in 1D),
+//   eps = min(eps0, rho_bar, p_bar); elements with an inadmissible average are kept;
+//   1. rho_min < eps:  rho <- rho_bar + theta1 (rho - rho_bar),
+//                      theta1 = (rho_bar - eps) / (rho_bar - rho_min);
+//   2. U <- Ubar + theta2 (U - Ubar), theta2 = min over nodes with p < eps of the
+//      point t of the segment Ubar -> U_q with pressure eps (60 bisection steps,
+//      keeping the admissible end).
+// It has no counterpart in the reference.  Elements that need no limiting are not
+// written back, so the pass reads the state once and writes only limited elements.
+//
+// 2D: one warp per element (lanes over its nodes, shuffles for the cell sums and
+// the minima); 1D: one thread per element.
+#include "pplimit.hpp"
+
+#include <cuda_runtime.h>
+
+namespace frsdg
+{
+namespace
+{
+
+__device__ __forceinline__ double pp_gas_pressure(const PPArgs& a, double rho, double e)
+{
+    if (a.gas_law == FRSDG_GAS_IDEAL) return (a.gas.gamma - 1.0) * rho * e;
+    const double covol = 1.0 - a.gas.b * rho;
+    const double cvT = e + a.gas.a * rho;
+    return ((a.gas.gamma - 1.0) * rho * cvT) / covol - a.gas.a * rho * rho;
+}
+
+template <int NV> __device__ __forceinline__ double pp_pressure(const PPArgs& a, const double* u)
+{
+    double m2 = 0.0;
+#pragma unroll
+    for (int c = 1; c < NV - 1; ++c) m2 += u[c] * u[c];
+    const double rho = u[0];
+    const double e = (u[NV - 1] - 0.5 * m2 / rho) / rho;
+    return pp_gas_pressure(a, rho, e);
+}
+
+template <int NV>
+__device__ __forceinline__ double pp_segment_root(const PPArgs& a, const double* ub, const double* uq, double eps)
+{
+    double lo = 0.0, hi = 1.0, s[NV];
+    for (int it = 0; it < 60; ++it)
+    {
+        const double mid = 0.5 * (lo + hi);
+#pragma unroll
+        for (int c = 0; c < NV; ++c) s[c] = ub[c] + mid * (uq[c] - ub[c]);
+        if (s[0] > 0.0 && pp_pressure<NV>(a, s) >= eps) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_min(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+template <int N> __global__ void __launch_bounds__(256) pp_limit2d_kernel(const PPArgs a)
+{
+    constexpr int NQ = N * N, R = (NQ + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    const int64_t e = int64_t(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32;
+    if (e >= a.nelem) return;  // whole warps leave together
+    double* base = a.U + e * (4 * NQ);
+    // the element's global row, for the cached detJ of a curved mesh (row windows wrap)
+    const int64_t j_loc = e / a.Nx;
+    const int64_t j_glob = ((j_loc + a.row_base) % a.Ny + a.Ny) % a.Ny;
+    const int64_t e_glob = j_glob * a.Nx + (e - j_loc * a.Nx);
+    double u[R][4], W[R];
+    double wsum = 0.0, ub[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+    {
+        const int q = lane + 32 * r;
+        W[r] = 0.0;
+        u[r][0] = u[r][1] = u[r][2] = u[r][3] = 0.0;
+        if (q < NQ)
+        {
+            const double2 x0 = *reinterpret_cast<const double2*>(base + q * 4);
+            const double2 x1 = *reinterpret_cast<const double2*>(base + q * 4 + 2);
+            u[r][0] = x0.x; u[r][1] = x0.y; u[r][2] = x1.x; u[r][3] = x1.y;
+            W[r] = a.w[q % N] * a.w[q / N] * (a.detJ ? __ldg(a.detJ + e_glob * NQ + q) : 1.0);
+        }
+        wsum += W[r];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) ub[c] += W[r] * u[r][c];
+    }
+    wsum = warp_sum(wsum);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) ub[c] = warp_sum(ub[c]) / wsum;
+    const double pb = pp_pressure<4>(a, ub);
+    if (!(ub[0] > 0.0) || !(pb > 0.0)) return;  // uniform across the warp
+    const double eps = fmin(a.eps0, fmin(ub[0], pb));
+    double rmin = 1e300;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (lane + 32 * r < NQ) rmin = fmin(rmin, u[r][0]);
+    rmin = warp_min(rmin);
+    bool touched = false;
+    if (rmin < eps)
+    {
+        const double th1 = (ub[0] - eps) / (ub[0] - rmin);
+#pragma unroll
+        for (int r = 0; r < R; ++r) u[r][0] = ub[0] + th1 * (u[r][0] - ub[0]);
+        touched = true;
+    }
+    double th2 = 1.0;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (lane + 32 * r < NQ && !(pp_pressure<4>(a, u[r]) >= eps)) th2 = fmin(th2, pp_segment_root<4>(a, ub, u[r], eps));
+    th2 = warp_min(th2);
+    if (th2 < 1.0)
+    {
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) u[r][c] = ub[c] + th2 * (u[r][c] - ub[c]);
+        touched = true;
+    }
+    if (!touched) return;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+    {
+        const int q = lane + 32 * r;
+        if (q >= NQ) continue;
+        *reinterpret_cast<double2*>(base + q * 4) = make_double2(u[r][0], u[r][1]);
+        *reinterpret_cast<double2*>(base + q * 4 + 2) = make_double2(u[r][2], u[r][3]);
+        if (a.U32)
+            *reinterpret_cast<float4*>(a.U32 + e * (4 * NQ) + q * 4) =
+                make_float4(float(u[r][0]), float(u[r][1]), float(u[r][2]), float(u[r][3]));
+    }
+}
+
+template <int N> __global__ void __launch_bounds__(128) pp_limit1d_kernel(const PPArgs a)
+{
+    const int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= a.nelem) return;
+    double* u = a.U + e * (3 * N);
+    double wsum = 0.0, ub[3] = {0.0, 0.0, 0.0};
+    for (int q = 0; q < N; ++q)
+    {
+        wsum += a.w[q];
+        for (int c = 0; c < 3; ++c) ub[c] += a.w[q] * u[c * N + q];
+    }
+    for (int c = 0; c < 3; ++c) ub[c] /= wsum;
+    const double pb = pp_pressure<3>(a, ub);
+    if (!(ub[0] > 0.0) || !(pb > 0.0)) return;
+    const double eps = fmin(a.eps0, fmin(ub[0], pb));
+    double rmin = u[0];
+    for (int q = 1; q < N; ++q) rmin = fmin(rmin, u[q]);
+    if (rmin < eps)
+    {
+        const double th1 = (ub[0] - eps) / (ub[0] - rmin);
+        for (int q = 0; q < N; ++q) u[q] = ub[0] + th1 * (u[q] - ub[0]);
+    }
+    double th2 = 1.0;
+    for (int q = 0; q < N; ++q)
+    {
+        const double uq[3] = {u[q], u[N + q], u[2 * N + q]};
+        if (!(pp_pressure<3>(a, uq) >= eps)) th2 = fmin(th2, pp_segment_root<3>(a, ub, uq, eps));
+    }
+    if (th2 < 1.0)
+        for (int q = 0; q < N; ++q)
+            for (int c = 0; c < 3; ++c) u[c * N + q] = ub[c] + th2 * (u[c * N + q] - ub[c]);
+}
+
+template <int N> cudaError_t launch_n(const PPArgs& a, cudaStream_t s)
+{
+    if (a.nelem <= 0) return cudaSuccess;
+    if (a.dim == 2)
+    {
+        const int64_t blocks = (a.nelem + 7) / 8;
+        pp_limit2d_kernel<N><<<unsigned(blocks), 256, 0, s>>>(a);
+    }
+    else
+    {
+        const int64_t blocks = (a.nelem + 127) / 128;
+        pp_limit1d_kernel<N><<<unsigned(blocks), 128, 0, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+} // namespace
+
+cudaError_t launch_pp_limit(const PPArgs& a, cudaStream_t s)
+{
+    switch (a.n)
+    {
+        case 2: return launch_n<2>(a, s);
+        case 3: return launch_n<3>(a, s);
+        case 4: return launch_n<4>(a, s);
+        case 5: return launch_n<5>(a, s);
+        case 6: return launch_n<6>(a, s);
+        case 7: return launch_n<7>(a, s);
+        case 8: return launch_n<8>(a, s);
+        case 9: return launch_n<9>(a, s);
+        case 10: return launch_n<10>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+} // namespace frsdg

@@ -10,8 +10,16 @@ and update in one pass over the state):
     U1 = U + dt L(U);  U2 = 3/4 U + 1/4 U1 + dt/4 L(U1);  U+ = 1/3 U + 2/3 U2 + 2 dt/3 L(U2)
   RK4 (classic):  acc accumulates dt/6 (k1 + 2 k2 + 2 k3 + k4) on top of U.
 
-Time step: dt = CFL * (L/N) / c_max(U0), c_max the largest |velocity| + sound speed
-of the initial state (tools/run_test_matrix.py:40-52 take c_max as an input).
+Time step (cfl_time_step): dt = CFL * (L/N) / c_max(U0), c_max the largest
+|velocity| + sound speed of the initial state (tools/run_test_matrix.py:40-52 take
+c_max as an input), or with rule "dg" dt = CFL * (L/N) / ((2p + 1) c_max(U0)), the
+(2p + 1)^-1 scaling of the explicit CFL ceilings that the reference's tools fit
+(tools/c-vcjh_claude.py:410-430, tools/cfl_ceiling_plots.py:110-130).
+
+With cfg.pp_limit the positivity limiter (frsdg_pp_limit) acts on every stage output
+and the post-step applies it after the stabilisation, as the Zhang-Shu scheme needs
+(J. Comput. Phys. 229 (2010) 8918-8934: SSP stages are convex combinations of Euler
+steps, each of which the limiter keeps admissible).
 """
 from __future__ import annotations
 
@@ -47,11 +55,16 @@ def max_wave_speed(cfg: A.frsdg_config, U: torch.Tensor) -> float:
     return float((torch.sqrt(u * u + v * v) + torch.sqrt(c2)).max())
 
 
-def cfl_time_step(cfg: A.frsdg_config, U0: torch.Tensor, cfl: float) -> float:
+def cfl_time_step(cfg: A.frsdg_config, U0: torch.Tensor, cfl: float, rule: str = "h") -> float:
+    """rule "h": CFL h / c_max; rule "dg": CFL h / ((2p + 1) c_max); h the smaller
+    element size."""
     h = cfg.box_length[0] / cfg.n_elems[0]
     if cfg.dim == 2:
         h = min(h, cfg.box_length[1] / cfg.n_elems[1])
-    return cfl * h / max_wave_speed(cfg, U0)
+    if rule not in ("h", "dg"):
+        raise ValueError("rule must be 'h' or 'dg'")
+    scale = 1.0 if rule == "h" else 1.0 / (2 * cfg.poly_deg + 1)
+    return cfl * scale * h / max_wave_speed(cfg, U0)
 
 
 @dataclass
@@ -84,6 +97,9 @@ class Integrator:
         self._buf = None
         cfg = solver.cfg
         self.stabilise = bool(cfg.apply_filter or cfg.apply_weno)
+        # the positivity limiter (cfg.pp_limit) acts on every stage output; the
+        # post-step applies it again after the stabilisation
+        self.pp = bool(cfg.pp_limit)
 
     def _buffers(self, U: torch.Tensor):
         if self._buf is None or self._buf[0].device != U.device:
@@ -96,17 +112,22 @@ class Integrator:
         s = self.s
         b1, b2, b3, u32, c1, c2 = self._buffers(U)
         u32.copy_(U)
+
+        def stage(tt, us32, out, out32, **kw):
+            s.rk_stage_mixed(tt, us32, out, out32, **kw)
+            if self.pp:
+                s.pp_limit(out, out32)
+
         if self.scheme == "ssprk3":
-            s.rk_stage_mixed(t, u32, b1, c1, gamma=dt, a=U, alpha=1.0)
-            s.rk_stage_mixed(t + dt, c1, b2, c2, gamma=0.25 * dt, a=U, alpha=0.75, b=b1, beta=0.25)
-            s.rk_stage_mixed(t + 0.5 * dt, c2, U, None, gamma=2.0 * dt / 3.0, a=U, alpha=1.0 / 3.0, b=b2,
-                             beta=2.0 / 3.0)
+            stage(t, u32, b1, c1, gamma=dt, a=U, alpha=1.0)
+            stage(t + dt, c1, b2, c2, gamma=0.25 * dt, a=U, alpha=0.75, b=b1, beta=0.25)
+            stage(t + 0.5 * dt, c2, U, None, gamma=2.0 * dt / 3.0, a=U, alpha=1.0 / 3.0, b=b2, beta=2.0 / 3.0)
         else:
             b3.copy_(U)
-            s.rk_stage_mixed(t, u32, b1, c1, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 6.0)
-            s.rk_stage_mixed(t + 0.5 * dt, c1, b2, c2, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
-            s.rk_stage_mixed(t + 0.5 * dt, c2, b1, c1, gamma=dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
-            s.rk_stage_mixed(t + dt, c1, U, None, gamma=dt / 6.0, a=b3, alpha=1.0)
+            stage(t, u32, b1, c1, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 6.0)
+            stage(t + 0.5 * dt, c1, b2, c2, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
+            stage(t + 0.5 * dt, c2, b1, c1, gamma=dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
+            stage(t + dt, c1, U, None, gamma=dt / 6.0, a=b3, alpha=1.0)
         if self.stabilise:
             s.apply_stabilization(U)
 
@@ -114,6 +135,8 @@ class Integrator:
         if self.before is not None:
             self.before(Us)
         self.s.rk_stage(t, Us, out, **kw)
+        if self.pp:
+            self.s.pp_limit(out)
 
     def step(self, U: torch.Tensor, t: float, dt: float) -> None:
         """Advance U (in place) from t to t + dt, then apply the post-step limiter."""

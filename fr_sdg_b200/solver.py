@@ -165,6 +165,15 @@ class FRSolver:
         self._check_vec(src, dst)
         A.check(self._lib.frsdg_post_step_to(self._h, _ptr(src), _ptr(dst), _stream()), "frsdg_post_step_to")
 
+    def pp_limit(self, U: torch.Tensor, U32: torch.Tensor | None = None) -> None:
+        """Positivity limiter on U in place (cfg.pp_limit; no counterpart in the
+        reference); U32, an FP32 copy of U, is refreshed where U changes."""
+        self._check_vec(U)
+        if U32 is not None:
+            self._check_f32(U32)
+        A.check(self._lib.frsdg_pp_limit(self._h, _ptr(U), _ptr(U32) if U32 is not None else None, _stream()),
+                "frsdg_pp_limit")
+
     def primitive_to_conservative(self, inp: torch.Tensor, out: torch.Tensor) -> None:
         self._check_vec(inp, out)
         A.check(self._lib.frsdg_prim_to_cons(self._h, _ptr(inp), _ptr(out), _stream()), "frsdg_prim_to_cons")

@@ -27,6 +27,7 @@ def make_config(dim: int = 2, p: int = 3, n_elems=(10, 10), box=(1.0, 1.0), rada
                 bcs=None, apply_filter: bool = False, cut_off: int = 2, strength: int = 32, alpha: float = 36.0,
                 apply_weno: bool = False, weno_gamma: float = 0.998, theta: float = 1.0, threshold: float = 0.8,
                 cond_sys: bool = False, csd_eps: float = 1e-7, coord_sys: int = A.COORD_CARTESIAN,
+                pp_limit: bool = False, pp_eps: float = 1e-13,
                 defaults: Callable[[A.frsdg_config], None] | None = None) -> A.frsdg_config:
     """Build a configuration; `bcs` maps a face (A.LEFT..A.BOTTOM) to a kind or
     to (kind, state, params).  The remaining fields take the library's defaults
@@ -63,6 +64,7 @@ def make_config(dim: int = 2, p: int = 3, n_elems=(10, 10), box=(1.0, 1.0), rada
     c.apply_filter, c.filt_cut_off, c.filt_strength, c.filt_alpha = int(apply_filter), cut_off, strength, alpha
     c.apply_weno, c.weno_gamma, c.shock_theta, c.shock_threshold = int(apply_weno), weno_gamma, theta, threshold
     c.cond_sys, c.csd_eps = int(cond_sys), csd_eps
+    c.pp_limit, c.pp_eps = int(pp_limit), pp_eps
     return c
 
 
@@ -159,6 +161,7 @@ class Workload:
     n_steps: int | None
     init: Callable[[str], torch.Tensor]
     notes: dict = field(default_factory=dict)
+    cfl_rule: str = "h"        # fr_sdg_b200.integrate.cfl_time_step
 
     @property
     def n_nodes(self) -> int:
@@ -171,22 +174,42 @@ class Workload:
     def n_dofs(self) -> int:
         return self.n_nodes * (self.cfg.dim + 2)
 
+    def time_step(self, U0: torch.Tensor) -> float:
+        """The workload's time step on the state U0 (its CFL number and rule)."""
+        from .integrate import cfl_time_step
 
-# Stabilisation of the shock runs.  The reference's factory puts the interface node at
-# x = 0.5 on the right state (factory.hpp:199), so the jump starts inside an element;
-# with the spectral filter alone the reference algorithm (and the oracle restating it)
-# produces NaN within the first steps at any CFL, and with filter and WENO both on the
-# WENO result is overwritten by the filter (filter.hpp:733-742).  Full runs therefore use
-# the reference tools' own shock settings: WENO with the shock sensor, filter off
-# (tools/check_radial.py:221-236), at a CFL below the explicit ceilings those tools
-# measured (tools/cfl_ceiling_shock.py:32-35).
+        return cfl_time_step(self.cfg, U0, self.cfl, self.cfl_rule)
+
+
+# Stabilisation of the shock workloads.  Their initial jumps sit inside elements (the
+# reference's factory puts the interface node on one state, factory.hpp:199), and the
+# reference's stabilisation keeps neither density nor pressure positive there: run
+# through fr_sdg's own code (oracle/_ref), the spectral filter alone makes the density
+# negative at the first post-step (removing the top Legendre mode of a step
+# overshoots), and WENO with the shock sensor loses positivity within 1-20 steps at
+# p >= 4 for every CFL number down to 0.0125 and every sensor setting tried.  The
+# shock workloads therefore keep the configured stabilisation and add the
+# positivity-preserving limiter (Zhang and Shu 2010; cfg.pp_limit) on every stage and
+# after the post-step, with the time step dt = CFL h / ((2p + 1) c_max): the (2p + 1)
+# scaling of the reference tools' own explicit CFL ceilings (tools/c-vcjh_claude.py:
+# 410-430, tools/cfl_ceiling_plots.py:110-130), which keeps CFL 0.1 below both the
+# linear stability limit of p >= 4 in 2D and the limiter's positivity bound
+# 1 / (2 p (p + 1)).
+FILTER_STAB = dict(apply_filter=True, pp_limit=True)
+# "spectral filter with a shock sensor active": filter and WENO + sensor both on; the
+# reference then keeps the filter's result in troubled elements (filter.hpp:733-742)
+FILTER_SENSOR_STAB = dict(apply_filter=True, apply_weno=True, weno_gamma=0.998, threshold=0.8, theta=1.0,
+                          pp_limit=True)
+# the reference tools' own shock-run settings (tools/check_radial.py:221-236): WENO with
+# the shock sensor, filter off
 SHOCK_STAB = dict(apply_filter=False, apply_weno=True, weno_gamma=0.998, threshold=0.8, theta=1.0)
 
 
 def sod1d(n_elems: int = 200, p: int = 3) -> Workload:
-    """1D Sod tube: [0,1], Rusanov, DG (c=0), SSP-RK3 to t_end 0.2, WENO + shock sensor."""
+    """1D Sod tube: [0,1], Rusanov, DG (c=0), SSP-RK3 to t_end 0.2, spectral filter on,
+    CFL 0.1 (dt = CFL h / ((2p+1) c_max)) with the positivity limiter."""
     cfg = make_config(dim=1, p=p, n_elems=(n_elems, 1), box=(1.0, 1.0), riemann="rusanov",
-                      bcs={A.LEFT: A.BC_OUTFLOW, A.RIGHT: A.BC_OUTFLOW}, **SHOCK_STAB)
+                      bcs={A.LEFT: A.BC_OUTFLOW, A.RIGHT: A.BC_OUTFLOW}, **FILTER_STAB)
 
     def init(device="cpu"):
         x, _ = node_coords(cfg, device)
@@ -196,7 +219,7 @@ def sod1d(n_elems: int = 200, p: int = 3) -> Workload:
         zero = torch.zeros_like(rho)
         return pack1d(rho, zero, rhoE("ideal", 1.4, 0, 0, rho, zero, p_))
 
-    return Workload(f"sod1d_n{n_elems}_p{p}", cfg, "ssprk3", 0.025, 0.2, None, init)
+    return Workload(f"sod1d_n{n_elems}_p{p}", cfg, "ssprk3", 0.1, 0.2, None, init, cfl_rule="dg")
 
 
 def vortex_curved(n_elems: int = 64, p: int = 4, amplitude: float = 0.1) -> Workload:
@@ -251,7 +274,8 @@ def bump_channel(nx: int = 256, ny: int = 64, p: int = 3, mach: float = 0.5) -> 
 def blast_large(n_elems: int = 1024, p: int = 5, ny: int | None = None, defaults=None,
                 gll_nodes=None) -> Workload:
     """2D radial blast on [0,1]^2, HLLC, Van der Waals (a=0.05, b=0.02, gamma=1.4),
-    SSP-RK3, 200 steps, WENO + shock sensor (CFL 0.01: p = 5).  ny > n_elems stacks
+    SSP-RK3, 200 steps, spectral filter with the shock sensor active and the positivity
+    limiter, CFL 0.1 (dt = CFL h / ((2p+1) c_max)).  ny > n_elems stacks
     more rows of the same element size above it (box [0,1] x [0, ny/n_elems]): the
     weak-scaling mesh of a row-block partition.  `defaults` and `gll_nodes` replace
     the library's configuration defaults and reference element (make_config,
@@ -262,7 +286,7 @@ def blast_large(n_elems: int = 1024, p: int = 5, ny: int | None = None, defaults
                       gas="vdw", gamma=g, vdw=(a, b),
                       bcs={A.LEFT: A.BC_OUTFLOW, A.RIGHT: A.BC_OUTFLOW, A.TOP: A.BC_OUTFLOW,
                            A.BOTTOM: A.BC_OUTFLOW},
-                      defaults=defaults, **SHOCK_STAB)
+                      defaults=defaults, **FILTER_SENSOR_STAB)
 
     def init(device="cpu", rows=None):
         x, y = node_coords(cfg, device, rows, gll_nodes)
@@ -273,18 +297,20 @@ def blast_large(n_elems: int = 1024, p: int = 5, ny: int | None = None, defaults
         zero = torch.zeros_like(rho)
         return pack2d(rho, zero, zero, rhoE("vdw", g, a, b, rho, zero, pr))
 
-    return Workload(f"blast_vdw_{n_elems}x{ny}_p{p}", cfg, "ssprk3", 0.01, None, 200, init)
+    return Workload(f"blast_vdw_{n_elems}x{ny}_p{p}", cfg, "ssprk3", 0.1, None, 200, init, cfl_rule="dg")
 
 
 def circular_explosion(n_elems: int, p: int, gas: str, gamma: float, vdw, r0: float, p_out: float,
                        filt_cut_off: int = 2) -> Workload:
     """One instance of the batched uneven workload: ProblemFactory2D<CircularExplosion>
-    (factory.hpp:400-465) on [-1,1]^2 with Rusanov and outflow boundaries."""
+    (factory.hpp:400-465) on [-1,1]^2 with Rusanov and outflow boundaries, spectral
+    filter on with the positivity limiter, SSP-RK3 to t_end 0.25 at CFL 0.1
+    (dt = CFL h / ((2p+1) c_max))."""
     cfg = make_config(dim=2, p=p, n_elems=(n_elems, n_elems), box=(2.0, 2.0), riemann="rusanov",
                       gas=gas, gamma=gamma, vdw=vdw,
                       bcs={A.LEFT: A.BC_OUTFLOW, A.RIGHT: A.BC_OUTFLOW, A.TOP: A.BC_OUTFLOW,
                            A.BOTTOM: A.BC_OUTFLOW},
-                      apply_filter=True, cut_off=filt_cut_off)
+                      cut_off=filt_cut_off, **FILTER_STAB)
 
     def init(device="cpu"):
         x, y = node_coords(cfg, device)
@@ -295,4 +321,4 @@ def circular_explosion(n_elems: int, p: int, gas: str, gamma: float, vdw, r0: fl
         zero = torch.zeros_like(rho)
         return pack2d(rho, zero, zero, rhoE(gas, gamma, vdw[0], vdw[1], rho, zero, pr))
 
-    return Workload(f"explosion_{n_elems}_p{p}_{gas}", cfg, "ssprk3", 0.1, 0.25, None, init)
+    return Workload(f"explosion_{n_elems}_p{p}_{gas}", cfg, "ssprk3", 0.1, 0.25, None, init, cfl_rule="dg")

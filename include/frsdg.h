@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define FRSDG_ABI_VERSION 1
+#define FRSDG_ABI_VERSION 2
 
 /* ---- status codes (PETSc-style: 0 = success) ---------------------------- */
 enum {
@@ -130,6 +130,14 @@ typedef struct frsdg_config {
                                 reference does (boundary_conditions.hpp:276-293); 1: they are
                                 differentiated too (exact Jacobian; 2D only) */
     double  csd_eps;         /* complex-step h (reference: 1e-7, petsc_solver_impl.hpp:179) */
+    /* positivity-preserving limiter (no counterpart in the reference): 1 = the
+     * scaling limiter of Zhang and Shu (J. Comput. Phys. 229, 2010) after the
+     * post-step stabilisation, and on every Runge-Kutta stage when frsdg_pp_limit is
+     * called there; cell averages by GLL quadrature, floor eps = min(pp_eps, rho_bar,
+     * p_bar).  Default 0 (off), pp_eps 1e-13. */
+    int32_t pp_limit;
+    int32_t pad1_;
+    double  pp_eps;
 } frsdg_config;
 
 typedef struct frsdg_handle frsdg_handle;
@@ -253,6 +261,16 @@ int frsdg_post_step(frsdg_handle* h, double* U, void* stream);
  * separate buffer limits it into the state directly, without the device copy of the
  * state that the in-place call makes for the WENO limiter. */
 int frsdg_post_step_to(frsdg_handle* h, const double* src, double* dst, void* stream);
+
+/* Positivity-preserving limiter on U in place (no counterpart in the reference):
+ * per element, scale the density about its cell average until rho >= eps, then the
+ * whole state until p >= eps (Zhang and Shu, J. Comput. Phys. 229 (2010) 8918-8934),
+ * eps = min(cfg.pp_eps, rho_bar, p_bar); elements already admissible are left
+ * untouched.  U32 (2D, may be NULL): an FP32 copy of U refreshed where U changes (the
+ * mixed-precision stage input).  Does nothing unless cfg.pp_limit.  frsdg_post_step and
+ * frsdg_post_step_to apply it after the stabilisation themselves; a time integrator
+ * calls it on the output of every Runge-Kutta stage. */
+int frsdg_pp_limit(frsdg_handle* h, double* U, float* U32, void* stream);
 
 /* cons = M(prim): PetscSolver::primitive_to_conservative (petsc_solver_impl.hpp:719-727). */
 int frsdg_prim_to_cons(frsdg_handle* h, const double* prim, double* cons, void* stream);

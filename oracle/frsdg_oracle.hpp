@@ -1359,4 +1359,101 @@ inline void post_step(const Problem& P, double* U)
         }
 }
 
+// ---------------------------------------------------------------- positivity limiter
+// The scaling limiter of Zhang and Shu (J. Comput. Phys. 229 (2010) 8918-8934,
+// sec. 3): per element, with the cell average Ubar taken by GLL quadrature (weights
+// w_k w_l detJ_kl in 2D, w_k in 1D) and eps = min(cfg.pp_eps, rho_bar, p_bar),
+//   1. rho_min < eps:  rho <- rho_bar + theta1 (rho - rho_bar),
+//                      theta1 = (rho_bar - eps) / (rho_bar - rho_min);
+//   2. p(U_q) < eps at some node: U <- Ubar + theta2 (U - Ubar), theta2 = min_q t_q,
+//      t_q in [0, 1) the point of the segment Ubar -> U_q where the pressure is eps,
+//      found by 60 bisection steps (p(Ubar + t d) >= eps keeps the lower end).
+// Elements whose average is itself inadmissible are left unchanged.  It has no
+// counterpart in the reference (cfg.pp_limit turns it on); the time integrators apply
+// it to every Runge-Kutta stage and after the post-step stabilisation.
+inline double pp_pressure(const Gas& g, int nv, const double* u)
+{
+    double m2 = 0.0;
+    for (int c = 1; c < nv - 1; ++c) m2 += u[c] * u[c];
+    const double rho = u[0];
+    const double e = (u[nv - 1] - 0.5 * m2 / rho) / rho;
+    return g.pressure(rho, e);
+}
+
+inline double pp_segment_root(const Gas& g, int nv, const double* ub, const double* uq, double eps)
+{
+    double lo = 0.0, hi = 1.0, s[4];
+    for (int it = 0; it < 60; ++it)
+    {
+        const double mid = 0.5 * (lo + hi);
+        for (int c = 0; c < nv; ++c) s[c] = ub[c] + mid * (uq[c] - ub[c]);
+        if (s[0] > 0.0 && pp_pressure(g, nv, s) >= eps) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// One element: nq nodes, value c of node q at u[q * sq + c * sc]; W[q] quadrature weights.
+inline void pp_limit_element(const Gas& g, int nv, int nq, const double* W, double* u, int sq, int sc, double eps0)
+{
+    double wsum = 0.0, ub[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int q = 0; q < nq; ++q)
+    {
+        wsum += W[q];
+        for (int c = 0; c < nv; ++c) ub[c] += W[q] * u[q * sq + c * sc];
+    }
+    for (int c = 0; c < nv; ++c) ub[c] /= wsum;
+    const double pb = pp_pressure(g, nv, ub);
+    if (!(ub[0] > 0.0) || !(pb > 0.0)) return;
+    const double eps = std::min(eps0, std::min(ub[0], pb));
+    double rmin = u[0];
+    for (int q = 1; q < nq; ++q) rmin = std::min(rmin, u[q * sq]);
+    if (rmin < eps)
+    {
+        const double th1 = (ub[0] - eps) / (ub[0] - rmin);
+        for (int q = 0; q < nq; ++q) u[q * sq] = ub[0] + th1 * (u[q * sq] - ub[0]);
+    }
+    double th2 = 1.0, uq[4];
+    for (int q = 0; q < nq; ++q)
+    {
+        for (int c = 0; c < nv; ++c) uq[c] = u[q * sq + c * sc];
+        if (!(pp_pressure(g, nv, uq) >= eps)) th2 = std::min(th2, pp_segment_root(g, nv, ub, uq, eps));
+    }
+    if (th2 < 1.0)
+        for (int q = 0; q < nq; ++q)
+            for (int c = 0; c < nv; ++c) u[q * sq + c * sc] = ub[c] + th2 * (u[q * sq + c * sc] - ub[c]);
+}
+
+inline void pp_limit(const Problem& P, double* U)
+{
+    const int n = P.n, nd = P.ndofs;
+    if (P.cfg.dim == 1)
+    {
+        for (int e = 0; e < P.Nx; ++e) pp_limit_element(P.gas, 3, n, P.re.w.data(), U + int64_t(e) * nd, 1, n, P.cfg.pp_eps);
+        return;
+    }
+    const bool curved = P.cfg.geometry == FRSDG_GEOM_SINE_WARP || P.cfg.geometry == FRSDG_GEOM_WALL_PROFILE;
+#pragma omp parallel for schedule(static) num_threads(P.nthreads)
+    for (int j = 0; j < P.Ny; ++j)
+    {
+        std::vector<double> W(size_t(n) * n);
+        for (int i = 0; i < P.Nx; ++i)
+        {
+            for (int l = 0; l < n; ++l)
+                for (int k = 0; k < n; ++k)
+                    W[size_t(l) * n + k] = P.re.w[k] * P.re.w[l] *
+                                           (curved ? P.metrics(P.comp_x(i, k), P.comp_y(j, l)).detJ : 1.0);
+            pp_limit_element(P.gas, 4, n * n, W.data(), U + (int64_t(j) * P.Nx + i) * nd, 4, 1, P.cfg.pp_eps);
+        }
+    }
+}
+
+// The post-step of this build: the reference's stabilisation, then (cfg.pp_limit) the
+// positivity limiter.
+inline void post_step_full(const Problem& P, double* U)
+{
+    if (P.cfg.apply_filter || P.cfg.apply_weno) post_step(P, U);
+    if (P.cfg.pp_limit) pp_limit(P, U);
+}
+
 } // namespace frsdg_oracle

@@ -43,6 +43,7 @@ def lib() -> C.CDLL:
             "oracle_ifunction": (C.c_int, [_P, _D, _P, _P, _P]),
             "oracle_jvp": (C.c_int, [_P, _D, _D, _P, _P, _P]),
             "oracle_post_step": (C.c_int, [_P, _P]),
+            "oracle_pp_limit": (C.c_int, [_P, _P]),
             "oracle_prim_to_cons": (C.c_int, [_P, _P, _P]),
             "oracle_reference_element": (C.c_int, [C.c_int, _D, _P, _P, _P, _P, _P]),
             "oracle_filter_matrix": (C.c_int, [C.c_int, C.c_int, C.c_int, _D, _P]),
@@ -130,6 +131,12 @@ class Oracle:
     def post_step(self, U) -> np.ndarray:
         U = self._vec(U).copy()
         _chk(lib().oracle_post_step(self._h, _p(U)), "oracle_post_step")
+        return U
+
+    def pp_limit(self, U) -> np.ndarray:
+        """The positivity limiter (cfg.pp_limit's stage limiter) applied to a copy of U."""
+        U = self._vec(U).copy()
+        _chk(lib().oracle_pp_limit(self._h, _p(U)), "oracle_pp_limit")
         return U
 
     def prim_to_cons(self, prim) -> np.ndarray:

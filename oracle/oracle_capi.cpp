@@ -81,7 +81,13 @@ int oracle_jvp(void* h, double t, double sigma, const double* U, const double* V
 
 int oracle_post_step(void* h, double* U)
 {
-    return guarded([&] { post_step(*static_cast<Problem*>(h), U); });
+    return guarded([&] { post_step_full(*static_cast<Problem*>(h), U); });
+}
+
+// The positivity limiter alone (applied to every Runge-Kutta stage).
+int oracle_pp_limit(void* h, double* U)
+{
+    return guarded([&] { pp_limit(*static_cast<Problem*>(h), U); });
 }
 
 int oracle_prim_to_cons(void* h, const double* prim, double* cons)

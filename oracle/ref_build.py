@@ -58,7 +58,8 @@ def build(reference: Path = DEFAULT_REFERENCE, force: bool = False, verbose: boo
     None when neither the reference nor a previously built library exists."""
     if not available(reference):
         return LIB if LIB.exists() else None
-    srcs = [HERE / "ref_capi.cpp", *sorted((HERE / "ref_shim").rglob("*")), HERE / "ref_build.py"]
+    srcs = [HERE / "ref_capi.cpp", *sorted((HERE / "ref_shim").rglob("*")), HERE / "ref_build.py",
+            HERE.parent / "include" / "frsdg.h"]
     inc = reference / "include"
     newest = max([p.stat().st_mtime for p in srcs if p.is_file()] + [p.stat().st_mtime for p in inc.glob("*.hpp")])
     if not force and LIB.exists() and LIB.stat().st_mtime >= newest:

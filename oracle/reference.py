@@ -166,6 +166,8 @@ def default_config(c) -> None:
     c.apply_filter, c.filt_cut_off, c.filt_strength, c.filt_alpha = 0, 2, 32, 36.0
     c.apply_weno, c.weno_gamma, c.shock_theta, c.shock_threshold = 0, 0.998, 1.0, 0.8
     c.cond_sys, c.jvp_exact_bc, c.csd_eps = 0, 0, 1e-7
+    # the positivity limiter has no counterpart in the reference: off, library floor
+    c.pp_limit, c.pp_eps = 0, 1e-13
 
 
 def reference_element(p: int, c: float = 0.0):

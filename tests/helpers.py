@@ -80,3 +80,21 @@ def cons_to_prim(cfg, U: np.ndarray) -> np.ndarray:
     u = q[:, 1] / rho
     e = q[:, 2] / rho - 0.5 * u * u
     return np.stack([np.log(rho), u, np.log(e)], axis=1).reshape(-1)
+
+
+def poisoned_state(cfg, seed: int, every: int = 3, gain: float = 4.0) -> np.ndarray:
+    """A seeded state whose cell averages are admissible but whose nodes are not in
+    every `every`-th element: there the deviations from the element's plain node mean
+    are amplified `gain` times, which drives nodal densities and pressures negative
+    (the input of the positivity limiter)."""
+    U = random_state(cfg, seed)
+    n = cfg.poly_deg + 1
+    if cfg.dim == 2:
+        q = U.reshape(-1, n * n, 4).copy()
+        m = q.mean(axis=1, keepdims=True)
+        q[::every] = m[::every] + gain * (q[::every] - m[::every])
+    else:
+        q = U.reshape(-1, 3, n).copy()
+        m = q.mean(axis=2, keepdims=True)
+        q[::every] = m[::every] + gain * (q[::every] - m[::every])
+    return q.reshape(-1)

@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
     out = subprocess.run(["nm", "-D", "--defined-only", str(A.LIB_PATH)], capture_output=True, text=True).stdout
     exported = set(re.findall(r"\bT (frsdg_[a-z0-9_]+)", out))
     assert set(declared_functions()) <= exported
-    assert lib.frsdg_abi_version() == 1
+    assert lib.frsdg_abi_version() == 2
 
 
 def test_struct_layout_matches_c(tmp_path):
@@ -72,6 +72,7 @@ def _create(cfg):
     (lambda c: setattr(c.bc[A.LEFT], "kind", A.BC_PERIODIC), A.ERR_ARG),  # only one side periodic
     (lambda c: (setattr(c, "apply_filter", 1), setattr(c, "filt_cut_off", 3)), A.ERR_ARG),  # 0/0 strength
     (lambda c: setattr(c, "csd_eps", 0.0), A.ERR_ARG),
+    (lambda c: (setattr(c, "pp_limit", 1), setattr(c, "pp_eps", 0.0)), A.ERR_ARG),
     (lambda c: setattr(c, "coord_sys", A.COORD_RADIAL), A.ERR_UNSUPPORTED),
 ])
 def test_invalid_configurations_rejected(mutate, code):

@@ -15,11 +15,12 @@ from fr_sdg_b200.integrate import Integrator
 class DecaySolver:
     """The rk_stage / apply_stabilization contract of FRSolver for dU/dt = -U."""
 
-    def __init__(self, limiter: bool):
-        self.cfg = SimpleNamespace(apply_filter=int(limiter), apply_weno=0, dim=2, cond_sys=0,
+    def __init__(self, limiter: bool, pp: bool = False):
+        self.cfg = SimpleNamespace(apply_filter=int(limiter), apply_weno=0, dim=2, cond_sys=0, pp_limit=int(pp),
                                    bc=[SimpleNamespace(kind=0) for _ in range(4)])
         self.stages = 0
         self.limits = 0
+        self.pp_calls = []
 
     def rk_stage(self, t, Us, out, gamma, a=None, alpha=0.0, b=None, beta=0.0, acc=None, delta=0.0):
         assert out.data_ptr() != Us.data_ptr()
@@ -36,6 +37,9 @@ class DecaySolver:
 
     def apply_stabilization(self, U):
         self.limits += 1
+
+    def pp_limit(self, U, U32=None):
+        self.pp_calls.append(U.data_ptr())
 
     def apply_stabilization_to(self, src, dst):
         assert src.data_ptr() != dst.data_ptr()
@@ -57,6 +61,21 @@ def test_stage_sequences_converge_at_their_order(scheme, order, limiter):
         errs.append(float((U - math.exp(-1.0)).abs().max()))
     rate = math.log2(errs[0] / errs[1])
     assert abs(rate - order) < 0.2, (errs, rate)
+
+
+@pytest.mark.parametrize("scheme", ["ssprk3", "rk4"])
+def test_positivity_limiter_acts_on_every_stage_output(scheme):
+    """cfg.pp_limit: the limiter runs on the output of every stage (Zhang-Shu needs
+    each Euler sub-step admissible), the last stage's output included."""
+    s = DecaySolver(limiter=True, pp=True)
+    U = torch.ones(8, dtype=torch.float64)
+    it = Integrator(s, scheme)
+    it.step(U, 0.0, 0.1)
+    assert len(s.pp_calls) == s.stages == (3 if scheme == "ssprk3" else 4)
+    assert s.limits == 1
+    s2 = DecaySolver(limiter=False, pp=False)
+    Integrator(s2, scheme).step(torch.ones(8, dtype=torch.float64), 0.0, 0.1)
+    assert s2.pp_calls == []
 
 
 def test_clipped_final_step_and_monitor_schedule():
@@ -100,7 +119,8 @@ def test_cfl_time_step_uniform_states():
     n_nodes = 3 * 2 * 16
     rho, u, v, p, g = 1.2, 0.3, -0.4, 0.9, 1.4
     for gas, (a, b) in (("ideal", (0.0, 0.0)), ("vdw", (0.05, 0.02))):
-        cfg = make_config(dim=2, p=3, n_elems=(3, 2), box=(0.6, 0.4), gas=gas, vdw=(a, b))
+        # element sizes 0.2 (x) and 0.1 (y): the time step takes the smaller one
+        cfg = make_config(dim=2, p=3, n_elems=(3, 2), box=(0.6, 0.2), gas=gas, vdw=(a, b))
         ones = torch.ones(n_nodes, dtype=torch.float64)
         E = rhoE(gas, g, a, b, rho * ones, (u * u + v * v) * ones, p * ones)
         U = pack2d(rho * ones, rho * u * ones, rho * v * ones, E)
@@ -113,4 +133,6 @@ def test_cfl_time_step_uniform_states():
             c = math.sqrt((g * (g - 1) * (e + a * rho) + (g - 1) * a * rho * (2 - b * rho)) / (cov * cov) - 2 * a * rho)
             # the state's pressure from the same gas law
             assert abs((g - 1) * rho * (e + a * rho) / cov - a * rho * rho - p) < 1e-12
-        assert abs(dt - 0.5 * 0.2 / (math.hypot(u, v) + c)) < 1e-12 * dt, gas
+        assert abs(dt - 0.5 * 0.1 / (math.hypot(u, v) + c)) < 1e-12 * dt, gas
+        # the "dg" rule divides by 2p + 1
+        assert abs(cfl_time_step(cfg, U, 0.5, "dg") - dt / 7.0) < 1e-12 * dt, gas

@@ -30,7 +30,7 @@ def oracle_run(cfg, U0: np.ndarray, dt: float, n_steps: int, scheme: str) -> np.
         out = out + gamma * v
         if acc is not None:
             acc += delta * v
-        return out
+        return o.pp_limit(out) if cfg.pp_limit else out
 
     U, t = U0.copy(), 0.0
     for _ in range(n_steps):
@@ -59,7 +59,7 @@ def test_run_matches_oracle_integrator(name, cuda):
     else:
         wl, steps = blast_large(n_elems=16, p=5), 10
     U0 = wl.init("cpu").numpy()
-    dt = cfl_time_step(wl.cfg, torch.from_numpy(U0), wl.cfl or 0.1)
+    dt = wl.time_step(torch.from_numpy(U0))
     scheme = "rk4" if wl.integrator == "rk4" else "ssprk3"
     ref = oracle_run(wl.cfg, U0, dt, steps, scheme)
     with FRSolver(wl.cfg) as s:
@@ -89,12 +89,12 @@ def test_vortex_converges_to_exact(cuda):
 
 
 def test_sod_against_exact_riemann(cuda):
-    """1D Sod tube (N = 200, p = 3, Rusanov, WENO + shock sensor, SSP-RK3) at t = 0.2 against
-    the exact Riemann solution: L1 density error small."""
+    """1D Sod tube (N = 200, p = 3, Rusanov, spectral filter + positivity limiter, SSP-RK3,
+    CFL 0.1) at t = 0.2 against the exact Riemann solution: L1 density error small."""
     wl = sod1d()
     with FRSolver(wl.cfg) as s:
         U = wl.init(cuda)
-        dt = cfl_time_step(wl.cfg, U, wl.cfl)
+        dt = wl.time_step(U)
         st = Integrator(s, "ssprk3").run(U, dt, t_end=wl.t_end)
         assert abs(st.t - 0.2) < 1e-12
         x, _ = node_coords(wl.cfg, "cpu")
@@ -114,7 +114,7 @@ def test_graph_replay_matches_eager(name, cuda):
         wl, scheme = sod1d(), "ssprk3"
     with FRSolver(wl.cfg) as s:
         U0 = wl.init(cuda)
-        dt = cfl_time_step(wl.cfg, U0, wl.cfl)
+        dt = wl.time_step(U0)
         Ue, Ug = U0.clone(), U0.clone()
         t_end = 25.5 * dt
         se = Integrator(s, scheme).run(Ue, dt, t_end=t_end)

@@ -57,7 +57,7 @@ def test_monitor_records_every_interval(cuda, tmp_path):
     wl = vortex_curved(n_elems=8, p=3)
     with FRSolver(wl.cfg) as s:
         U0 = wl.init(cuda)
-        dt = cfl_time_step(wl.cfg, U0, wl.cfl)
+        dt = wl.time_step(U0)
         ref, U = [U0.clone()], U0.clone()
         it = Integrator(s, "rk4")
         for k in range(5):
@@ -80,7 +80,7 @@ def test_monitor_final_only_with_graph(cuda, tmp_path):
     wl = sod1d()
     with FRSolver(wl.cfg) as s:
         U0 = wl.init(cuda)
-        dt = cfl_time_step(wl.cfg, U0, wl.cfl)
+        dt = wl.time_step(U0)
         t_end = 20.5 * dt
         Ue, Ug = U0.clone(), U0.clone()
         Integrator(s, "ssprk3").run(Ue, dt, t_end=t_end)
