@@ -82,6 +82,8 @@ SIGNATURES = {
     "frsdg_pp_limit": (C.c_int, [_P, _P, _P, _P]),
     "frsdg_rhs_host": (C.c_int, [_P, _D, _P, _P, _P]),
     "frsdg_status": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "frsdg_check_state": (C.c_int, [_P, _P, _P]),
+    "frsdg_device_math": (C.c_int, [C.c_int32, _P, _P, C.c_int64, _P]),
     "frsdg_petsc_vec_record_bytes": (C.c_int, [C.c_int64, C.c_int32, C.POINTER(C.c_int64)]),
     "frsdg_petsc_vec_pack": (C.c_int, [_P, C.c_int64, C.c_int32, _P, _P]),
     "frsdg_reference_element": (C.c_int, [C.c_int32, _D, _P, _P, _P, _P, _P]),

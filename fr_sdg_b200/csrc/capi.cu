@@ -1061,6 +1061,24 @@ int frsdg_rhs_host(frsdg_handle* h, double t, const double* U_host, double* rhs_
     return FRSDG_OK;
 }
 
+int frsdg_check_state(frsdg_handle* h, const double* U, void* stream)
+{
+    if (!h || !U) return fail(FRSDG_ERR_ARG, "null argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    h->last = s;
+    const cudaError_t e = launch_check_density(h->cfg.dim, h->n, local_nelem(h), U, h->d_bad, s);
+    if (e != cudaSuccess) return cuda_fail(e, "state-check launch");
+    return FRSDG_OK;
+}
+
+int frsdg_device_math(int32_t op, const double* x, double* y, int64_t n, void* stream)
+{
+    if ((op != 0 && op != 1) || n < 0 || (n > 0 && (!x || !y))) return fail(FRSDG_ERR_ARG, "bad argument");
+    const cudaError_t e = launch_device_math(op, x, y, n, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "device-math launch");
+    return FRSDG_OK;
+}
+
 int frsdg_status(frsdg_handle* h, int64_t* bad_nodes)
 {
     if (!h || !bad_nodes) return fail(FRSDG_ERR_ARG, "null argument");

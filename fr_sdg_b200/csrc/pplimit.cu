@@ -15,6 +15,7 @@
 // 2D: one warp per element (lanes over its nodes, shuffles for the cell sums and
 // the minima); 1D: one thread per element.
 #include "pplimit.hpp"
+#include "device_math.cuh"
 
 #include <cuda_runtime.h>
 
@@ -194,7 +195,53 @@ template <int N> cudaError_t launch_n(const PPArgs& a, cudaStream_t s)
     return cudaGetLastError();
 }
 
+// Health check of a state: nodes whose density is not positive and finite, added to
+// the handle's health word (one atomic per warp that found any).
+__global__ void __launch_bounds__(256) check_density_kernel(const double* U, int64_t nodes, int stride_node,
+                                                            int stride_elem, int per_elem, unsigned long long* bad)
+{
+    const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    bool b = false;
+    if (q < nodes)
+    {
+        const int64_t e = q / per_elem, k = q - e * per_elem;
+        const double rho = __ldg(U + e * stride_elem + k * stride_node);
+        b = !(rho > 0.0) || !(rho < 1e308);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, b);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(bad, (unsigned long long)__popc(m));
+}
+
+// The library's device reciprocal and square root (device_math.cuh), elementwise, for
+// validation against IEEE division and sqrt.
+__global__ void device_math_kernel(int op, const double* x, double* y, int64_t n)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    y[i] = op == 0 ? s_rcp(x[i]) : s_sqrt(x[i]);
+}
+
 } // namespace
+
+cudaError_t launch_check_density(int dim, int n, int64_t nelem, const double* U, unsigned long long* bad,
+                                 cudaStream_t s)
+{
+    const int per_elem = dim == 2 ? n * n : n;
+    const int64_t nodes = nelem * per_elem;
+    if (nodes <= 0) return cudaSuccess;
+    // 2D: density of node q at q*4 (node-major AoS); 1D: eq 0 of element e at e*3n + k
+    const int stride_node = dim == 2 ? 4 : 1, stride_elem = dim == 2 ? 4 * n * n : 3 * n;
+    check_density_kernel<<<unsigned((nodes + 255) / 256), 256, 0, s>>>(U, nodes, stride_node, stride_elem,
+                                                                        per_elem, bad);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_device_math(int op, const double* x, double* y, int64_t n, cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    device_math_kernel<<<unsigned((n + 255) / 256), 256, 0, s>>>(op, x, y, n);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_pp_limit(const PPArgs& a, cudaStream_t s)
 {

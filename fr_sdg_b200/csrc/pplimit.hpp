@@ -20,5 +20,10 @@ struct PPArgs
 };
 
 cudaError_t launch_pp_limit(const PPArgs& a, cudaStream_t s);
+// nodes of U (nelem elements) whose density is not positive and finite, added to *bad
+cudaError_t launch_check_density(int dim, int n, int64_t nelem, const double* U, unsigned long long* bad,
+                                 cudaStream_t s);
+// y = s_rcp(x) (op 0) or s_sqrt(x) (op 1), elementwise
+cudaError_t launch_device_math(int op, const double* x, double* y, int64_t n, cudaStream_t s);
 
 } // namespace frsdg

@@ -72,6 +72,7 @@ class RunStats:
     steps: int
     t: float
     dt: float
+    rejected: int = 0  # steps rejected on the health word and retried as two half steps
 
 
 class Integrator:
@@ -187,14 +188,42 @@ class Integrator:
         cur.wait_stream(side)
         return g
 
+    def _guarded_step(self, U: torch.Tensor, t: float, dt: float, depth: int, max_reject: int) -> int:
+        """One step with rejection (PETSc's -ts_max_reject, tools/c-vcjh_test.py:100-105):
+        the step is taken from a saved copy of U; if the health word then reports a node
+        with non-positive or non-finite density (in the stage inputs, read by the
+        residuals, or in the result, read by frsdg_check_state), U is restored and the
+        step is retried as two steps of dt/2, at most max_reject halvings deep.
+        Returns the number of rejections."""
+        while len(self._saved) <= depth:
+            self._saved.append(torch.empty_like(U))
+        saved = self._saved[depth]
+        saved.copy_(U)
+        self.s.status()  # clear the health word
+        self.step(U, t, dt)
+        self.s.check_state(U)
+        if self.s.status() == 0:
+            return 0
+        if depth >= max_reject:
+            raise RuntimeError(f"step at t = {t:.6g} failed after {max_reject} halvings of dt")
+        U.copy_(saved)
+        r = self._guarded_step(U, t, 0.5 * dt, depth + 1, max_reject)
+        r += self._guarded_step(U, t + 0.5 * dt, 0.5 * dt, depth + 1, max_reject)
+        return r + 1
+
     def run(self, U: torch.Tensor, dt: float, t_end: float | None = None, n_steps: int | None = None,
-            t0: float = 0.0, graph: bool = False, steps_per_graph: int = 64, monitor=None) -> RunStats:
+            t0: float = 0.0, graph: bool = False, steps_per_graph: int = 64, monitor=None,
+            max_reject: int = 0) -> RunStats:
         """March to t_end (last step clipped to land on it) or for n_steps steps.  With
         graph=True (and a residual that does not read t) the full steps replay a CUDA
         graph of `steps_per_graph` steps; leftover and clipped steps run eagerly.
         monitor(step, t, U, final) is called with the initial state (step 0) and after
         every step (petsc_io.SolutionMonitor writes the PETSc solution file); a monitor
-        that writes intermediate steps keeps the run eager."""
+        that writes intermediate steps keeps the run eager.  max_reject > 0: every step
+        checks the health word and a failed step is retried with halved steps
+        (_guarded_step); such runs are eager and synchronise once per step."""
+        if max_reject > 0:
+            return self._run_guarded(U, dt, t_end, n_steps, t0, monitor, max_reject)
         tol = 1e-14 * max(1.0, abs(t_end)) if t_end is not None else 0.0
         if t_end is not None:
             n_full = 0
@@ -234,6 +263,23 @@ class Integrator:
             if monitor is not None:
                 monitor(k, t, U, True)
         return RunStats(k, t, dt)
+
+    def _run_guarded(self, U, dt, t_end, n_steps, t0, monitor, max_reject) -> RunStats:
+        self._saved = []
+        tol = 1e-14 * max(1.0, abs(t_end)) if t_end is not None else 0.0
+        t, k, rej = t0, 0, 0
+        if monitor is not None:
+            monitor(0, t0, U, False)
+        while (n_steps is None or k < n_steps) and (t_end is None or t < t_end - tol):
+            h = dt if t_end is None else min(dt, t_end - t)
+            rej += self._guarded_step(U, t, h, 0, max_reject)
+            t = t + h if t_end is None or t + h < t_end - tol else t_end
+            k += 1
+            if monitor is not None:
+                done = (n_steps is not None and k >= n_steps) or (t_end is not None and t >= t_end - tol)
+                monitor(k, t, U, done)
+        self._saved = []
+        return RunStats(k, t, dt, rej)
 
 
 def node_jacobian(cfg: A.frsdg_config, device="cpu") -> torch.Tensor:

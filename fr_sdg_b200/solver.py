@@ -185,6 +185,12 @@ class FRSolver:
                 raise ValueError("expected contiguous float64 host vectors")
         A.check(self._lib.frsdg_rhs_host(self._h, t, _ptr(U_host), _ptr(rhs_host), _stream()), "frsdg_rhs_host")
 
+    def check_state(self, U: torch.Tensor) -> None:
+        """Count the nodes of U with non-positive or non-finite density into the health
+        word (read by status())."""
+        self._check_vec(U)
+        A.check(self._lib.frsdg_check_state(self._h, _ptr(U), _stream()), "frsdg_check_state")
+
     def status(self) -> int:
         """Nodes with non-positive or non-finite density seen since the last call."""
         n = C.c_int64()

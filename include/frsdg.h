@@ -287,6 +287,19 @@ int frsdg_rhs_host(frsdg_handle* h, double t, const double* U_host, double* rhs_
  * stream. */
 int frsdg_status(frsdg_handle* h, int64_t* bad_nodes);
 
+/* Add to the health word the nodes of U whose density is not positive and finite
+ * (read back by frsdg_status).  The residual calls count the states they read; this
+ * check covers a state that no residual has read yet, such as the output of the last
+ * stage of a step: the time integrator's step rejection (the reference leaves it to
+ * PETSc, -ts_max_reject, tools/c-vcjh_test.py:100-105) reads both. */
+int frsdg_check_state(frsdg_handle* h, const double* U, void* stream);
+
+/* The library's device FP64 reciprocal (op 0) and square root (op 1) -- a
+ * single-precision seed refined by Newton steps, used throughout the residual --
+ * applied elementwise to the device array x[0..n) into y, for validation against
+ * IEEE division and sqrt.  No handle needed. */
+int frsdg_device_math(int32_t op, const double* x, double* y, int64_t n, void* stream);
+
 /* Largest solution (in doubles) frsdg_post_step_static accepts: 4,194,304 (32 MiB
  * of scratch held on every device that loads the library). */
 #define FRSDG_POST_STEP_STATIC_MAX_DOFS 4194304

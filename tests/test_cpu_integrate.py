@@ -34,12 +34,25 @@ class DecaySolver:
             acc += delta * v
         out.copy_(o + gamma * v)
         self.stages += 1
+        if gamma > self.unstable_above:
+            self._bad += 1
 
     def apply_stabilization(self, U):
         self.limits += 1
 
     def pp_limit(self, U, U32=None):
         self.pp_calls.append(U.data_ptr())
+
+    # health word: a stage with gamma above `unstable_above` "goes bad"
+    unstable_above = float("inf")
+    _bad = 0
+
+    def check_state(self, U):
+        pass
+
+    def status(self):
+        b, self._bad = self._bad, 0
+        return b
 
     def apply_stabilization_to(self, src, dst):
         assert src.data_ptr() != dst.data_ptr()
@@ -76,6 +89,29 @@ def test_positivity_limiter_acts_on_every_stage_output(scheme):
     s2 = DecaySolver(limiter=False, pp=False)
     Integrator(s2, scheme).step(torch.ones(8, dtype=torch.float64), 0.0, 0.1)
     assert s2.pp_calls == []
+
+
+def test_step_rejection_halves_failed_steps():
+    """max_reject: a step whose health word reports bad nodes is undone and retaken as two
+    half steps (PETSc's -ts_max_reject); the result is the one of the half steps."""
+    s = DecaySolver(limiter=False)
+    s.unstable_above = 0.06  # the first SSP-RK3 stage has gamma = dt
+    U = torch.ones(4, dtype=torch.float64)
+    st = Integrator(s, "ssprk3").run(U, 0.1, t_end=1.0, max_reject=3)
+    assert st.steps == 10 and st.rejected == 10 and abs(st.t - 1.0) < 1e-14
+    g = lambda h: 1 - h + h * h / 2 - h ** 3 / 6
+    assert abs(float(U[0]) - g(0.05) ** 20) < 1e-14
+    # two levels: dt = 0.2 fails, 0.1 fails, 0.05 passes
+    s2 = DecaySolver(limiter=False)
+    s2.unstable_above = 0.06
+    U2 = torch.ones(4, dtype=torch.float64)
+    st2 = Integrator(s2, "ssprk3").run(U2, 0.2, t_end=0.4, max_reject=3)
+    assert st2.steps == 2 and st2.rejected == 2 * 3 and abs(float(U2[0]) - g(0.05) ** 8) < 1e-14
+    # a step that no halving rescues
+    s3 = DecaySolver(limiter=False)
+    s3.unstable_above = 0.001
+    with pytest.raises(RuntimeError):
+        Integrator(s3, "ssprk3").run(torch.ones(4, dtype=torch.float64), 0.1, n_steps=2, max_reject=2)
 
 
 def test_clipped_final_step_and_monitor_schedule():
