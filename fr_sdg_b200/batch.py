@@ -86,6 +86,18 @@ def instance_workload(spec: InstanceSpec, stab: str = "filter") -> Workload:
     return wl
 
 
+def density_l2(cfg, U: torch.Tensor, V: torch.Tensor) -> float:
+    """GLL-quadrature L2 norm of the density difference of two states of one instance
+    (physical measure: detJ of the affine map, (h_x/2)(h_y/2))."""
+    from .refelem import reference_element
+
+    n = cfg.poly_deg + 1
+    w = torch.tensor(reference_element(cfg.poly_deg)[1], dtype=torch.float64, device=U.device)
+    jac = (0.5 * cfg.box_length[0] / cfg.n_elems[0]) * (0.5 * cfg.box_length[1] / cfg.n_elems[1])
+    d = (U.view(-1, n, n, 4)[..., 0] - V.view(-1, n, n, 4)[..., 0])
+    return float(torch.sqrt(jac * ((w[:, None] * w[None, :])[None] * d * d).sum()))
+
+
 @dataclass
 class BatchResult:
     instances: int
@@ -100,15 +112,20 @@ class BatchResult:
 class BatchedInstances:
     """All instances of a batch, resident on one GPU."""
 
-    def __init__(self, specs: list[InstanceSpec], device, stab: str = "filter", streams: int = 16, init=None):
-        """init(cfg, device) -> state replaces the explosion initial states (tests)."""
+    def __init__(self, specs: list[InstanceSpec], device, stab: str = "filter", streams: int = 16, init=None,
+                 mixed: bool = False, pp_eps: float | None = None):
+        """init(cfg, device) -> state replaces the explosion initial states (tests).
+        mixed: FP32 residuals with FP64 stage sums (Integrator(mixed=True)).
+        pp_eps: the positivity limiter's floor, replacing the workload's."""
         self.device = torch.device(device)
         self.items = []
         for sp in specs:
             wl = instance_workload(sp, stab)
+            if pp_eps is not None:
+                wl.cfg.pp_eps = pp_eps
             s = FRSolver(wl.cfg)
             U = wl.init(self.device) if init is None else init(wl.cfg, self.device)
-            self.items.append((wl, s, U, Integrator(s, "ssprk3")))
+            self.items.append((wl, s, U, Integrator(s, "ssprk3", mixed=mixed)))
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(streams)]
 
     @property

@@ -9,6 +9,7 @@
 #include "frsdg_internal.hpp"
 #include "setup_ops.hpp"
 #include "jacobi.hpp"
+#include "handle.hpp"
 #include "pplimit.hpp"
 #include "stab.hpp"
 
@@ -130,9 +131,6 @@ int report(int code, const char* msg) { return fail(code, msg); }
 int report_cuda(cudaError_t e, const char* what) { return cuda_fail(e, what); }
 } // namespace frsdg
 
-struct frsdg_handle
-{
-    frsdg_config cfg{};
     int          n = 0, Nx = 0, Ny = 0, ndofs = 0;
     int64_t      ntot = 0, nelem = 0;
     int          geo = GEO_AFFINE;
@@ -521,6 +519,7 @@ int frsdg_create(const frsdg_config* cfg, frsdg_handle** out)
         p.row_base = 0;
         for (int q = 0; q < n; ++q) p.w[q] = h->re.w[q];
         p.detJ = h->d_detJ;
+        p.enabled = cfg->pp_limit;
     }
 
     // post-step stabilisation

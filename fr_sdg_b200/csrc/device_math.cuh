@@ -134,6 +134,13 @@ __device__ __forceinline__ cplx s_wrap_positive(cplx r)
 
 template <class S> __device__ __forceinline__ S s_select(bool c, S a, S b) { return c ? a : b; }
 
+// The health word's test of a density: positive and finite.  Positive finite doubles
+// (subnormals included) are exactly the bit patterns 1 .. 0x7fefffffffffffff.
+__device__ __forceinline__ bool density_ok(double rho)
+{
+    return static_cast<unsigned long long>(__double_as_longlong(rho)) - 1ull < 0x7fefffffffffffffull;
+}
+
 template <class S> struct scalar_traits;
 template <> struct scalar_traits<double>
 {

@@ -106,6 +106,46 @@ struct Fr2dArgs
     Ops    ops;
 };
 
+// ---- batches of instances (batch.cu) ----------------------------------------
+// Clock of one instance of a batch: the device-side time loop of frsdg_batch_run.
+// One step takes h = dt, or the remainder t_end - t when a full step would overshoot
+// (by more than 1e-14 relative), and the instance stays active while t < t_end.
+struct BatchClock
+{
+    double t, dt, t_end;
+    int    active, pad_;
+};
+
+__host__ __device__ inline double batch_step_size(const BatchClock& c)
+{
+    const double tol = 1e-14 * (c.t_end > 1.0 ? c.t_end : (c.t_end < -1.0 ? -c.t_end : 1.0));
+    return c.t + c.dt <= c.t_end + tol ? c.dt : c.t_end - c.t;
+}
+
+// One instance of a batch group: its residual launch template (the operators are the
+// group's) and its state and stage buffers.
+struct BatchInst2D
+{
+    Fr2dArgs a;
+    double*  U;       // state
+    double*  b[3];    // SSP-RK3 stage outputs (b[2]: the last, limited into U by the post-step)
+    float*   u32;     // mixed form: FP32 copy of U ...
+    float*   c[2];    // ... and of the first two stage outputs
+    int      inst;    // batch index (clock)
+    int      pad_;
+};
+
+struct Fr2dBatchArgs
+{
+    Ops ops;
+    const BatchInst2D* inst;
+    const BatchClock*  clock;
+    const int4*        tiles;  // (instance in group, bx, by, -)
+    int ntiles;
+    int stage;                 // SSP-RK3 stage 0, 1, 2
+    int mixed;
+};
+
 // Colour of element (gi, gj) for the coloured Jacobian: no two elements sharing a
 // face have the same colour.  Checkerboard, or, when a periodic direction has an
 // odd number of elements, (i mod 2 | 2 for the last) + 3 (j mod 2 | 2 for the last).
@@ -168,6 +208,9 @@ __host__ __device__ constexpr int tile_y(int n, int words, bool f32)
 // Launchers (one translation unit per polynomial order).
 template <class S, int N> cudaError_t launch_fr2d(int gas, int riem, int geo, const Fr2dArgs& a, cudaStream_t s);
 template <class S, int N> cudaError_t launch_fr1d(int gas, int riem, const Fr1dArgs& a, cudaStream_t s);
+template <class S, int N>
+cudaError_t launch_fr2d_batch(int gas, int riem, int var, const Fr2dBatchArgs& b, int grid, cudaStream_t s,
+                              int* occupancy);
 
 // Output of one real residual value r = R at index idx in the requested form.
 __device__ __forceinline__ void store_residual(int mode, const double* W, const StageArgs& st, double* out,

@@ -15,4 +15,6 @@ template cudaError_t launch_fr2d<cplx, FRSDG_N>(int, int, int, const Fr2dArgs&, 
 template cudaError_t launch_fr2d<float, FRSDG_N>(int, int, int, const Fr2dArgs&, cudaStream_t);
 template cudaError_t launch_fr1d<double, FRSDG_N>(int, int, const Fr1dArgs&, cudaStream_t);
 template cudaError_t launch_fr1d<cplx, FRSDG_N>(int, int, const Fr1dArgs&, cudaStream_t);
+template cudaError_t launch_fr2d_batch<double, FRSDG_N>(int, int, int, const Fr2dBatchArgs&, int, cudaStream_t, int*);
+template cudaError_t launch_fr2d_batch<float, FRSDG_N>(int, int, int, const Fr2dBatchArgs&, int, cudaStream_t, int*);
 } // namespace frsdg

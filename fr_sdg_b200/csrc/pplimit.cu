@@ -70,17 +70,15 @@ __device__ __forceinline__ double warp_min(double v)
     return v;
 }
 
-template <int N> __global__ void __launch_bounds__(256) pp_limit2d_kernel(const PPArgs a)
+// One element of a 2D state, limited by one warp: base / base32 point at the element's
+// values (base32 may be null), e_glob is its global index for the cached detJ;
+// refresh32: write the FP32 copy even when the element is admissible.
+template <int N>
+__device__ __forceinline__ void pp_element2d(const PPArgs& a, double* base, float* base32, int64_t e_glob,
+                                             bool limit, bool refresh32)
 {
     constexpr int NQ = N * N, R = (NQ + 31) / 32;
     const int lane = threadIdx.x & 31;
-    const int64_t e = int64_t(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32;
-    if (e >= a.nelem) return;  // whole warps leave together
-    double* base = a.U + e * (4 * NQ);
-    // the element's global row, for the cached detJ of a curved mesh (row windows wrap)
-    const int64_t j_loc = e / a.Nx;
-    const int64_t j_glob = ((j_loc + a.row_base) % a.Ny + a.Ny) % a.Ny;
-    const int64_t e_glob = j_glob * a.Nx + (e - j_loc * a.Nx);
     double u[R][4], W[R];
     double wsum = 0.0, ub[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
@@ -104,45 +102,104 @@ template <int N> __global__ void __launch_bounds__(256) pp_limit2d_kernel(const 
 #pragma unroll
     for (int c = 0; c < 4; ++c) ub[c] = warp_sum(ub[c]) / wsum;
     const double pb = pp_pressure<4>(a, ub);
-    if (!(ub[0] > 0.0) || !(pb > 0.0)) return;  // uniform across the warp
-    const double eps = fmin(a.eps0, fmin(ub[0], pb));
-    double rmin = 1e300;
-#pragma unroll
-    for (int r = 0; r < R; ++r)
-        if (lane + 32 * r < NQ) rmin = fmin(rmin, u[r][0]);
-    rmin = warp_min(rmin);
     bool touched = false;
-    if (rmin < eps)
+    // the limiter acts when enabled and the cell average is admissible (uniform across the warp)
+    if (limit && ub[0] > 0.0 && pb > 0.0)
     {
-        const double th1 = (ub[0] - eps) / (ub[0] - rmin);
-#pragma unroll
-        for (int r = 0; r < R; ++r) u[r][0] = ub[0] + th1 * (u[r][0] - ub[0]);
-        touched = true;
-    }
-    double th2 = 1.0;
-#pragma unroll
-    for (int r = 0; r < R; ++r)
-        if (lane + 32 * r < NQ && !(pp_pressure<4>(a, u[r]) >= eps)) th2 = fmin(th2, pp_segment_root<4>(a, ub, u[r], eps));
-    th2 = warp_min(th2);
-    if (th2 < 1.0)
-    {
+        const double eps = fmin(a.eps0, fmin(ub[0], pb));
+        double rmin = 1e300;
 #pragma unroll
         for (int r = 0; r < R; ++r)
+            if (lane + 32 * r < NQ) rmin = fmin(rmin, u[r][0]);
+        rmin = warp_min(rmin);
+        if (rmin < eps)
+        {
+            const double th1 = (ub[0] - eps) / (ub[0] - rmin);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) u[r][c] = ub[c] + th2 * (u[r][c] - ub[c]);
-        touched = true;
+            for (int r = 0; r < R; ++r) u[r][0] = ub[0] + th1 * (u[r][0] - ub[0]);
+            touched = true;
+        }
+        double th2 = 1.0;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (lane + 32 * r < NQ && !(pp_pressure<4>(a, u[r]) >= eps)) th2 = fmin(th2, pp_segment_root<4>(a, ub, u[r], eps));
+        th2 = warp_min(th2);
+        if (th2 < 1.0)
+        {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) u[r][c] = ub[c] + th2 * (u[r][c] - ub[c]);
+            touched = true;
+        }
     }
-    if (!touched) return;
+    if (!touched && !refresh32) return;
 #pragma unroll
     for (int r = 0; r < R; ++r)
     {
         const int q = lane + 32 * r;
         if (q >= NQ) continue;
-        *reinterpret_cast<double2*>(base + q * 4) = make_double2(u[r][0], u[r][1]);
-        *reinterpret_cast<double2*>(base + q * 4 + 2) = make_double2(u[r][2], u[r][3]);
-        if (a.U32)
-            *reinterpret_cast<float4*>(a.U32 + e * (4 * NQ) + q * 4) =
+        if (touched)
+        {
+            *reinterpret_cast<double2*>(base + q * 4) = make_double2(u[r][0], u[r][1]);
+            *reinterpret_cast<double2*>(base + q * 4 + 2) = make_double2(u[r][2], u[r][3]);
+        }
+        if (base32)
+            *reinterpret_cast<float4*>(base32 + q * 4) =
                 make_float4(float(u[r][0]), float(u[r][1]), float(u[r][2]), float(u[r][3]));
+    }
+}
+
+template <int N> __global__ void __launch_bounds__(256) pp_limit2d_kernel(const PPArgs a)
+{
+    constexpr int NQ = N * N;
+    const int64_t e = int64_t(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32;
+    if (e >= a.nelem) return;  // whole warps leave together
+    // the element's global row, for the cached detJ of a curved mesh (row windows wrap)
+    const int64_t j_loc = e / a.Nx;
+    const int64_t j_glob = ((j_loc + a.row_base) % a.Ny + a.Ny) % a.Ny;
+    const int64_t e_glob = j_glob * a.Nx + (e - j_loc * a.Nx);
+    pp_element2d<N>(a, a.U + e * (4 * NQ), a.U32 ? a.U32 + e * (4 * NQ) : nullptr, e_glob, true, false);
+}
+
+template <int N> __global__ void __launch_bounds__(256) pp_batch_kernel(const PPBatchArgs b)
+{
+    constexpr int NQ = N * N;
+    const int64_t g = int64_t(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32;
+    if (g >= b.nelem) return;  // whole warps leave together
+    int lo = 0, hi = b.ninst;  // instance i with elem_begin[i] <= g < elem_begin[i + 1]
+    while (hi - lo > 1)
+    {
+        const int mid = (lo + hi) / 2;
+        if (b.elem_begin[mid] <= g) lo = mid;
+        else hi = mid;
+    }
+    const BatchInst2D& in = b.binst[lo];
+    if (!b.clock[in.inst].active) return;
+    const PPArgs& a = b.inst[lo];
+    const int64_t e = g - b.elem_begin[lo];
+    double* buf = b.slot == 3 ? in.U : in.b[b.slot];
+    float* buf32 = !b.mixed ? nullptr : b.slot == 3 ? in.u32 : b.slot < 2 ? in.c[b.slot] : nullptr;
+    if (!a.enabled && !(b.slot == 3 && buf32)) return;
+    pp_element2d<N>(a, buf + e * (4 * NQ), buf32 ? buf32 + e * (4 * NQ) : nullptr, 0, a.enabled != 0,
+                    b.slot == 3 && buf32);
+}
+
+__global__ void batch_clock_kernel(BatchClock* clock, int count, int* active_count)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count)
+    {
+        BatchClock c = clock[i];
+        if (c.active)
+        {
+            const double h = batch_step_size(c);
+            c.t = h == c.dt ? c.t + c.dt : c.t_end;
+            const double tol = 1e-14 * (c.t_end > 1.0 ? c.t_end : (c.t_end < -1.0 ? -c.t_end : 1.0));
+            c.active = c.t < c.t_end - tol;
+            clock[i] = c;
+        }
+        if (c.active && active_count) atomicAdd(active_count, 1);
     }
 }
 
@@ -177,6 +234,13 @@ template <int N> __global__ void __launch_bounds__(128) pp_limit1d_kernel(const 
     if (th2 < 1.0)
         for (int q = 0; q < N; ++q)
             for (int c = 0; c < 3; ++c) u[c * N + q] = ub[c] + th2 * (u[c * N + q] - ub[c]);
+}
+
+template <int N> cudaError_t launch_pp_batch_n(const PPBatchArgs& b, cudaStream_t s)
+{
+    if (b.nelem <= 0) return cudaSuccess;
+    pp_batch_kernel<N><<<unsigned((b.nelem + 7) / 8), 256, 0, s>>>(b);
+    return cudaGetLastError();
 }
 
 template <int N> cudaError_t launch_n(const PPArgs& a, cudaStream_t s)
@@ -222,6 +286,30 @@ __global__ void device_math_kernel(int op, const double* x, double* y, int64_t n
 }
 
 } // namespace
+
+cudaError_t launch_pp_batch(int n, const PPBatchArgs& b, cudaStream_t s)
+{
+    switch (n)
+    {
+        case 2: return launch_pp_batch_n<2>(b, s);
+        case 3: return launch_pp_batch_n<3>(b, s);
+        case 4: return launch_pp_batch_n<4>(b, s);
+        case 5: return launch_pp_batch_n<5>(b, s);
+        case 6: return launch_pp_batch_n<6>(b, s);
+        case 7: return launch_pp_batch_n<7>(b, s);
+        case 8: return launch_pp_batch_n<8>(b, s);
+        case 9: return launch_pp_batch_n<9>(b, s);
+        case 10: return launch_pp_batch_n<10>(b, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_batch_clock(BatchClock* clock, int count, int* active_count, cudaStream_t s)
+{
+    if (count <= 0) return cudaSuccess;
+    batch_clock_kernel<<<(count + 255) / 256, 256, 0, s>>>(clock, count, active_count);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_check_density(int dim, int n, int64_t nelem, const double* U, unsigned long long* bad,
                                  cudaStream_t s)

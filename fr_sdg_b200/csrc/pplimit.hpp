@@ -17,7 +17,26 @@ struct PPArgs
     const double* detJ;     // 2D curved meshes: detJ per node [global elem][l n + k]; null: constant
     double*   U;            // state, limited in place
     float*    U32;          // optional FP32 copy of U, refreshed where U changes (2D)
+    int       enabled;      // cfg.pp_limit
+    int       pad_;
 };
+
+// Positivity limiter over a batch group (affine 2D instances of one order): warp per
+// element of the group's concatenated elements; the slot picks the buffer.
+struct PPBatchArgs
+{
+    const PPArgs*      inst;        // per instance in the group
+    const BatchInst2D* binst;       // their buffers
+    const int64_t*     elem_begin;  // first element of each instance, ninst + 1 entries
+    int                ninst;
+    int64_t            nelem;
+    const BatchClock*  clock;
+    int                slot;        // 0: b[0] (+c[0]), 1: b[1] (+c[1]), 2: b[2], 3: U (+u32 everywhere when mixed)
+    int                mixed;
+};
+cudaError_t launch_pp_batch(int n, const PPBatchArgs& b, cudaStream_t s);
+// advance the clocks of a batch by one step; count the instances still active
+cudaError_t launch_batch_clock(BatchClock* clock, int count, int* active_count, cudaStream_t s);
 
 cudaError_t launch_pp_limit(const PPArgs& a, cudaStream_t s);
 // nodes of U (nelem elements) whose density is not positive and finite, added to *bad

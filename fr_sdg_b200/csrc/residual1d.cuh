@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(kThreads) fr1d_kernel(const Fr1dArgs a)
         const int e = q / N, node = q % N;
         const S* u = sU + (e + 1) * ND;
         S s[3] = {u[node], u[N + node], u[2 * N + node]};
-        if (!(s_re(s[0]) > 0.0) && a.bad) atomicAdd(a.bad, 1ull);
+        if (!density_ok(s_re(s[0])) && a.bad) atomicAdd(a.bad, 1ull);
         S F[3], p, rw, ee;
         flux1<GAS>(g, s, F, p, rw, ee);
         for (int eq = 0; eq < 3; ++eq) sF[e * ND + eq * N + node] = F[eq];

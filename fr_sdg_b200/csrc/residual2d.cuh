@@ -17,6 +17,8 @@
 // The derivative matrix is read from the kernel-parameter constant bank with
 // compile-time indices; tile loops have compile-time trip counts.
 #pragma once
+#include <cstddef>
+
 #include "device_math.cuh"
 #include "frsdg_internal.hpp"
 #include "physics.cuh"
@@ -70,12 +72,14 @@ __host__ __device__ constexpr int reg_cap(int n, int words, bool f32, int bt)
 #endif
 }
 
-template <class S, int N, int GEO> struct Tile2D
+// VAR selects the tile: 0 the tuned shape of tile_x/tile_y, 1 the same tile with half
+// the element rows (fewer elements per CTA; a candidate of the batch autotuner).
+template <class S, int N, int GEO, int VAR = 0> struct Tile2D
 {
     static constexpr int W  = scalar_traits<S>::words;
     static constexpr bool F32 = sizeof(S) == 4;
     static constexpr int TX = tile_x(N, W, F32);
-    static constexpr int TY = tile_y(N, W, F32);
+    static constexpr int TY = VAR == 0 || tile_y(N, W, F32) == 1 ? tile_y(N, W, F32) : tile_y(N, W, F32) / 2;
     static constexpr int NN = N * N;
     static constexpr int TE = TX * TY;
     static constexpr bool JVP = scalar_traits<S>::words == 2;
@@ -225,11 +229,10 @@ template <class S> struct FaceSide
 
 // Locate face point t of the x-faces (XF) or y-faces of the tile, fetch both
 // side records.  Returns false (with harmless records) when t is not a face point.
-template <class S, int N, int GEO, bool XF>
+template <class S, int N, int GEO, bool XF, class T>
 __device__ __forceinline__ bool face_prepare(const Fr2dArgs& a, bool exists, int t, int i0, int j0, int txe,
                                              int tye, const S* sRec, FaceSide<S> sd[2])
 {
-    using T = Tile2D<S, N, GEO>;
     constexpr int TX = T::TX, NREC = T::NREC;
     const int pos = t % N, r = t / N;
     int face, row, lim;
@@ -296,10 +299,10 @@ __device__ __forceinline__ bool face_prepare(const Fr2dArgs& a, bool exists, int
 }
 
 // Replace the record of a boundary side by its ghost (rare path).
-template <int GAS, class S, int N, bool XF>
+template <int GAS, class S, int N, bool XF, class T>
 __device__ __forceinline__ void face_ghost(const Fr2dArgs& a, int i0, int j0, FaceSide<S> sd[2])
 {
-    constexpr int TX = Tile2D<S, N, GEO_AFFINE>::TX, NN = N * N;
+    constexpr int TX = T::TX, NN = N * N;
 #pragma unroll
     for (int side = 0; side < 2; ++side)
     {
@@ -318,11 +321,11 @@ __device__ __forceinline__ void face_ghost(const Fr2dArgs& a, int i0, int j0, Fa
 
 // Jumps scale*(F* - F.n) of the tile sides of a face point; F.n from the cached
 // volume fluxes (F.n = F on affine x-faces, G on affine y-faces).
-template <class S, int N, int GEO, bool XF>
+template <class S, int N, int GEO, bool XF, class T>
 __device__ __forceinline__ void face_jumps(const Fr2dArgs& a, int i0, int j0, bool valid, const FaceSide<S> sd[2],
                                            const S Fs[4], const S* sF, const S* sG, S* sDel)
 {
-    constexpr int TX = Tile2D<S, N, GEO_AFFINE>::TX, NN = N * N;
+    constexpr int TX = T::TX, NN = N * N;
     using R_t = typename scalar_traits<S>::real;
     if (!valid) return;
 #pragma unroll
@@ -355,15 +358,16 @@ __device__ __forceinline__ void face_jumps(const Fr2dArgs& a, int i0, int j0, bo
     }
 }
 
-template <class S, int N, int GAS, int RIEM, int GEO>
-__global__ void __launch_bounds__((Tile2D<S, N, GEO>::BT)) __maxnreg__((Tile2D<S, N, GEO>::MAXREG))
-fr2d_kernel(const __grid_constant__ Fr2dArgs a)
+// One tile of the residual pass: tile (bx, by) of element columns/rows (the Jacobian
+// slice of MODE_JAC is blockIdx.z), with the launch arguments `a` and the operators
+// `ops`; smem_raw is the CTA's dynamic shared memory (T::bytes).
+template <class S, int N, int GAS, int RIEM, int GEO, int VAR>
+__device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int bx, int by, unsigned char* smem_raw)
 {
-    using T = Tile2D<S, N, GEO>;
+    using T = Tile2D<S, N, GEO, VAR>;
     constexpr int TX = T::TX, TY = T::TY, NN = T::NN, TE = T::TE, BT = T::BT, NREC = T::NREC;
     using R_t = typename scalar_traits<S>::real;
     constexpr int ND = 4 * NN;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     S* sm   = reinterpret_cast<S*>(smem_raw);
     S* sF   = sm + T::oF;
     S* sG   = sm + T::oG;
@@ -374,7 +378,7 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
 
     const int tid = threadIdx.x;
     const int Nx = a.Nx, Ny = a.Ny;
-    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY + a.row_begin;
+    const int i0 = bx * TX, j0 = by * TY + a.row_begin;
     const int txe = min(TX, Nx - i0), tye = min(TY, a.row_end - j0);
     const GasParams g = a.gas;
 
@@ -471,7 +475,7 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
 #pragma unroll
                 for (int eq = 0; eq < 4; ++eq) sSeed[(e * 4 + eq) * NN + node] = s_im(s[eq]);
             }
-            if (!(s_re(s[0]) > 0.0) && a.bad) atomicAdd(a.bad, 1ull);
+            if (!density_ok(s_re(s[0])) && a.bad) atomicAdd(a.bad, 1ull);
             const NodePrim<S> pr = node_prim<GAS>(g, s[0], s[1], s[2], s[3]);
             const S rEp = s[3] + pr.p;
             const S ruv = s[1] * pr.v;
@@ -541,8 +545,8 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
 #pragma unroll
                 for (int m = 0; m < N; ++m)
                 {
-                    dG = dG + opD<R_t>(a.ops, l * N + m) * gv[m];
-                    dF = dF + opD<R_t>(a.ops, l * N + m) * fv[m];
+                    dG = dG + opD<R_t>(ops, l * N + m) * gv[m];
+                    dF = dF + opD<R_t>(ops, l * N + m) * fv[m];
                 }
                 const double2 me = __ldg(reinterpret_cast<const double2*>(mt + l * N * 4));
                 sC[(e * 4 + eq) * NN + l * N + k] = R_t(me.x) * dF + R_t(me.y) * dG;
@@ -555,7 +559,7 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
             {
                 S dG = S(0.0);
 #pragma unroll
-                for (int m = 0; m < N; ++m) dG = dG + opD<R_t>(a.ops, l * N + m) * gv[m];
+                for (int m = 0; m < N; ++m) dG = dG + opD<R_t>(ops, l * N + m) * gv[m];
                 sC[(e * 4 + eq) * NN + l * N + k] = R_t(a.eta_y) * dG;
             }
         }
@@ -570,18 +574,18 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
             S Fs[4];
             if (xf)
             {
-                if (face_prepare<S, N, GEO, true>(a, t < NXF, t, i0, j0, txe, tye, sRec, sd))
+                if (face_prepare<S, N, GEO, true, T>(a, t < NXF, t, i0, j0, txe, tye, sRec, sd))
                 {
-                    if (sd[0].bc || sd[1].bc) face_ghost<GAS, S, N, true>(a, i0, j0, sd);
+                    if (sd[0].bc || sd[1].bc) face_ghost<GAS, S, N, true, T>(a, i0, j0, sd);
                     riemann_rec<RIEM>(sd[0].R, sd[1].R, sd[0].nx, sd[0].ny, Fs);
-                    face_jumps<S, N, GEO, true>(a, i0, j0, true, sd, Fs, sF, sG, sDel);
+                    face_jumps<S, N, GEO, true, T>(a, i0, j0, true, sd, Fs, sF, sG, sDel);
                 }
             }
-            else if (face_prepare<S, N, GEO, false>(a, t < NYF, t, i0, j0, txe, tye, sRec, sd))
+            else if (face_prepare<S, N, GEO, false, T>(a, t < NYF, t, i0, j0, txe, tye, sRec, sd))
             {
-                if (sd[0].bc || sd[1].bc) face_ghost<GAS, S, N, false>(a, i0, j0, sd);
+                if (sd[0].bc || sd[1].bc) face_ghost<GAS, S, N, false, T>(a, i0, j0, sd);
                 riemann_rec<RIEM>(sd[0].R, sd[1].R, sd[0].nx, sd[0].ny, Fs);
-                face_jumps<S, N, GEO, false>(a, i0, j0, true, sd, Fs, sF, sG, sDel);
+                face_jumps<S, N, GEO, false, T>(a, i0, j0, true, sd, Fs, sF, sG, sDel);
             }
         }
         else
@@ -596,16 +600,16 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
             if (t < PFP)
             {
                 FaceSide<S> xs[2], ys[2];
-                const bool vx = face_prepare<S, N, GEO, true>(a, t < NXF, t, i0, j0, txe, tye, sRec, xs);
-                const bool vy = face_prepare<S, N, GEO, false>(a, t < NYF, t, i0, j0, txe, tye, sRec, ys);
+                const bool vx = face_prepare<S, N, GEO, true, T>(a, t < NXF, t, i0, j0, txe, tye, sRec, xs);
+                const bool vy = face_prepare<S, N, GEO, false, T>(a, t < NYF, t, i0, j0, txe, tye, sRec, ys);
                 if (!vx && !vy) continue;
-                if (xs[0].bc || xs[1].bc) face_ghost<GAS, S, N, true>(a, i0, j0, xs);
-                if (ys[0].bc || ys[1].bc) face_ghost<GAS, S, N, false>(a, i0, j0, ys);
+                if (xs[0].bc || xs[1].bc) face_ghost<GAS, S, N, true, T>(a, i0, j0, xs);
+                if (ys[0].bc || ys[1].bc) face_ghost<GAS, S, N, false, T>(a, i0, j0, ys);
                 S Fx[4], Fy[4];
                 riemann_rec<RIEM>(xs[0].R, xs[1].R, xs[0].nx, xs[0].ny, Fx);
                 riemann_rec<RIEM>(ys[0].R, ys[1].R, ys[0].nx, ys[0].ny, Fy);
-                face_jumps<S, N, GEO, true>(a, i0, j0, vx, xs, Fx, sF, sG, sDel);
-                face_jumps<S, N, GEO, false>(a, i0, j0, vy, ys, Fy, sF, sG, sDel);
+                face_jumps<S, N, GEO, true, T>(a, i0, j0, vx, xs, Fx, sF, sG, sDel);
+                face_jumps<S, N, GEO, false, T>(a, i0, j0, vy, ys, Fy, sF, sG, sDel);
             }
             else if (t - PFP < NCOL)
                 column(t - PFP);
@@ -623,7 +627,7 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
         S fv[N];
 #pragma unroll
         for (int m = 0; m < N; ++m) fv[m] = Fr[m];
-        const R_t dLl = opL<R_t>(a.ops, l), dRl = opR<R_t>(a.ops, l);
+        const R_t dLl = opL<R_t>(ops, l), dRl = opR<R_t>(ops, l);
         const S dxl = sDel[((e * 4 + 0) * 4 + eq) * N + l];
         const S dxr = sDel[((e * 4 + 1) * 4 + eq) * N + l];
         const S* dyb = sDel + ((e * 4 + 2) * 4 + eq) * N;
@@ -650,13 +654,13 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
         {
             S dF = S(0.0);
 #pragma unroll
-            for (int m = 0; m < N; ++m) dF = dF + opD<R_t>(a.ops, k * N + m) * fv[m];
+            for (int m = 0; m < N; ++m) dF = dF + opD<R_t>(ops, k * N + m) * fv[m];
             S R;
             if constexpr (GEO == GEO_CURVED)
             {
                 S dG = S(0.0);
 #pragma unroll
-                for (int m = 0; m < N; ++m) dG = dG + opD<R_t>(a.ops, k * N + m) * gr[m];
+                for (int m = 0; m < N; ++m) dG = dG + opD<R_t>(ops, k * N + m) * gr[m];
                 const double2 mx = __ldg(reinterpret_cast<const double2*>(
                     a.metrics + ((int64_t(j0 + ty + a.row_base) * Nx + (i0 + tx)) * NN + l * N + k) * 4));
                 R = (R_t(mx.x) * dF + R_t(mx.y) * dG) + sC[(e * 4 + eq) * NN + l * N + k];
@@ -666,8 +670,8 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
                 const S px = R_t(a.xi_x) * dF;
                 R = px + sC[(e * 4 + eq) * NN + l * N + k];
             }
-            R = R + dxl * opL<R_t>(a.ops, k);
-            R = R + dxr * opR<R_t>(a.ops, k);
+            R = R + dxl * opL<R_t>(ops, k);
+            R = R + dxr * opR<R_t>(ops, k);
             R = R + dyb[k] * dLl;
             R = R + dyt[k] * dRl;
             const int64_t gidx = gbase + (l * N + k) * 4;
@@ -688,6 +692,14 @@ fr2d_kernel(const __grid_constant__ Fr2dArgs a)
             }
         }
     }
+}
+
+template <class S, int N, int GAS, int RIEM, int GEO>
+__global__ void __launch_bounds__((Tile2D<S, N, GEO>::BT)) __maxnreg__((Tile2D<S, N, GEO>::MAXREG))
+fr2d_kernel(const __grid_constant__ Fr2dArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    fr2d_tile<S, N, GAS, RIEM, GEO, 0>(a, a.ops, blockIdx.x, blockIdx.y, smem_raw);
 }
 
 template <class S, int N, int GAS, int RIEM, int GEO>
@@ -712,6 +724,128 @@ cudaError_t launch_fr2d_kernel(const Fr2dArgs& a, cudaStream_t st)
               a.mode == MODE_JAC ? (a.jac_cmode == 2 ? 5 : a.jac_cmode ? 9 : 2) * T::NN * 4 : 1);
     kern<<<grid, T::BT, T::bytes, st>>>(a);
     return cudaGetLastError();
+}
+
+// ---- batches ------------------------------------------------------------------
+// Stage k of SSP-RK3 (Shu and Osher) for instance `in` at its own clock, in the form the
+// integrator's stages take (fr_sdg_b200/integrate.py):
+//   k = 0: b0 = U + h L(U);  k = 1: b1 = 3/4 U + 1/4 b0 + h/4 L(b0);
+//   k = 2: b2 = 1/3 U + 2/3 b1 + 2h/3 L(b1);  the mixed form reads the FP32 copies.
+__device__ __forceinline__ void batch_stage_args(Fr2dArgs& a, const BatchInst2D& in, const BatchClock& ck, int k,
+                                                 bool mixed)
+{
+    const double h = batch_step_size(ck);
+    a.mode = MODE_STAGE;
+    a.cond_sys = 0;
+    a.out_f32 = 0;
+    a.W = nullptr;
+    a.st.acc = nullptr;
+    a.st.delta = 0.0;
+    a.st.A = in.U;
+    if (k == 0)
+    {
+        a.U = mixed ? reinterpret_cast<const double*>(in.u32) : in.U;
+        a.out = in.b[0];
+        a.st.B = nullptr;
+        a.st.alpha = 1.0;
+        a.st.beta = 0.0;
+        a.st.gamma = h;
+        a.st.out32 = mixed ? in.c[0] : nullptr;
+        a.t = ck.t;
+    }
+    else if (k == 1)
+    {
+        a.U = mixed ? reinterpret_cast<const double*>(in.c[0]) : in.b[0];
+        a.out = in.b[1];
+        a.st.B = in.b[0];
+        a.st.alpha = 0.75;
+        a.st.beta = 0.25;
+        a.st.gamma = 0.25 * h;
+        a.st.out32 = mixed ? in.c[1] : nullptr;
+        a.t = ck.t + h;
+    }
+    else
+    {
+        a.U = mixed ? reinterpret_cast<const double*>(in.c[1]) : in.b[1];
+        a.out = in.b[2];
+        a.st.B = in.b[1];
+        a.st.alpha = 1.0 / 3.0;
+        a.st.beta = 2.0 / 3.0;
+        a.st.gamma = 2.0 * h / 3.0;
+        a.st.out32 = nullptr;
+        a.t = ck.t + 0.5 * h;
+    }
+}
+
+// One SSP-RK3 stage of a batch group: persistent CTAs walk the group's tile list
+// (instance in group, bx, by), copy the instance's launch arguments (all but the
+// operators, which are the group's) into shared memory and run the residual tile with
+// the stage epilogue.  Inactive instances (clock) are skipped.
+template <class S, int N, int GAS, int RIEM, int VAR>
+__global__ void __launch_bounds__((Tile2D<S, N, GEO_AFFINE, VAR>::BT)) __maxnreg__((Tile2D<S, N, GEO_AFFINE, VAR>::MAXREG))
+fr2d_batch_kernel(const __grid_constant__ Fr2dBatchArgs b)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(16) unsigned long long sa_raw[(sizeof(Fr2dArgs) + 7) / 8];
+    Fr2dArgs& sa = *reinterpret_cast<Fr2dArgs*>(sa_raw);
+    constexpr int HEAD = int(offsetof(Fr2dArgs, ops) / 8);  // the arguments before the operators
+    for (int tile = blockIdx.x; tile < b.ntiles; tile += gridDim.x)
+    {
+        const int4 tm = b.tiles[tile];
+        const BatchInst2D& in = b.inst[tm.x];
+        const BatchClock ck = b.clock[in.inst];
+        if (!ck.active) continue;  // uniform over the CTA
+        __syncthreads();           // the previous tile is done with sa and the tile memory
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&in.a);
+        for (int q = threadIdx.x; q < HEAD; q += blockDim.x) sa_raw[q] = src[q];
+        __syncthreads();
+        if (threadIdx.x == 0) batch_stage_args(sa, in, ck, b.stage, b.mixed != 0);
+        __syncthreads();
+        fr2d_tile<S, N, GAS, RIEM, GEO_AFFINE, VAR>(sa, b.ops, tm.y, tm.z, smem_raw);
+    }
+}
+
+template <class S, int N, int GAS, int RIEM, int VAR>
+cudaError_t launch_fr2d_batch_kernel(const Fr2dBatchArgs& b, int grid, cudaStream_t st, int* occupancy)
+{
+    using T = Tile2D<S, N, GEO_AFFINE, VAR>;
+    auto kern = fr2d_batch_kernel<S, N, GAS, RIEM, VAR>;
+    static bool attr_done[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !attr_done[dev])
+    {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(T::bytes));
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) attr_done[dev] = true;
+    }
+    if (occupancy) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, kern, T::BT, T::bytes);
+    if (grid > 0 && b.ntiles > 0) kern<<<grid, T::BT, T::bytes, st>>>(b);
+    return cudaGetLastError();
+}
+
+// Batched stage launcher of one order N (affine geometry): grid CTAs, or with
+// `occupancy` set only the number of CTAs of the variant that fit on one SM.
+template <class S, int N>
+cudaError_t launch_fr2d_batch(int gas, int riem, int var, const Fr2dBatchArgs& b, int grid, cudaStream_t s,
+                              int* occupancy)
+{
+    const int key = (gas * 2 + riem) * 2 + (var ? 1 : 0);
+    switch (key)
+    {
+        case 0: return launch_fr2d_batch_kernel<S, N, 0, 0, 0>(b, grid, s, occupancy);
+        case 1: return launch_fr2d_batch_kernel<S, N, 0, 0, 1>(b, grid, s, occupancy);
+        case 2: return launch_fr2d_batch_kernel<S, N, 0, 1, 0>(b, grid, s, occupancy);
+        case 3: return launch_fr2d_batch_kernel<S, N, 0, 1, 1>(b, grid, s, occupancy);
+        case 4: return launch_fr2d_batch_kernel<S, N, 1, 0, 0>(b, grid, s, occupancy);
+        case 5: return launch_fr2d_batch_kernel<S, N, 1, 0, 1>(b, grid, s, occupancy);
+        case 6: return launch_fr2d_batch_kernel<S, N, 1, 1, 0>(b, grid, s, occupancy);
+        case 7: return launch_fr2d_batch_kernel<S, N, 1, 1, 1>(b, grid, s, occupancy);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 template <class S, int N> cudaError_t launch_fr2d(int gas, int riem, int geo, const Fr2dArgs& a, cudaStream_t s)

@@ -137,17 +137,16 @@ template <int N> __device__ __forceinline__ double line_smoothness(const StabArg
 // |x|^theta; theta = 1 (the shock runs' setting) is exactly |x|
 __device__ __forceinline__ double sensor_pow(double x, double theta) { return theta == 1.0 ? x : pow(x, theta); }
 
-// three CTAs per SM at n <= 6 (shared memory allows three there)
-template <int N> __global__ void __launch_bounds__(kThreads, N <= 6 ? 3 : 1) stab2d_tile_kernel(const StabArgs a)
+// One tile (bx, by) of the 2D post-step; stab_smem is the CTA's dynamic shared memory.
+template <int N> __device__ __forceinline__ void stab2d_tile(const StabArgs& a, int bx, int by, unsigned char* stab_smem)
 {
     using T = StabTile<N>;
     constexpr int TX = T::TX, TY = T::TY, TE = T::TE, ND = T::ND, LX = T::LX;
-    extern __shared__ __align__(16) unsigned char stab_smem[];
     double* sU = reinterpret_cast<double*>(stab_smem);
     double* sX = sU + T::NSLOT * ND;
     double* sB = sX + TE * ND;
     const int tid = threadIdx.x;
-    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+    const int i0 = bx * TX, j0 = by * TY;
     const int txe = min(TX, a.Nx - i0), tye = min(TY, a.Ny - j0);
     const bool weno = a.apply_weno && !a.apply_filter;
     const int nslot = weno ? T::NSLOT : TE;
@@ -333,6 +332,31 @@ template <int N> __global__ void __launch_bounds__(kThreads, N <= 6 ? 3 : 1) sta
     }
 }
 
+// three CTAs per SM at n <= 6 (shared memory allows three there)
+template <int N> __global__ void __launch_bounds__(kThreads, N <= 6 ? 3 : 1) stab2d_tile_kernel(const StabArgs a)
+{
+    extern __shared__ __align__(16) unsigned char stab_smem[];
+    stab2d_tile<N>(a, blockIdx.x, blockIdx.y, stab_smem);
+}
+
+// The post-step of a batch group: tile t of the list is (instance in group, bx, by);
+// the instance's arguments come from device memory into shared memory, inactive
+// instances (clock) are skipped.
+template <int N> __global__ void __launch_bounds__(kThreads, N <= 6 ? 3 : 1) stab2d_batch_kernel(const StabBatchArgs b)
+{
+    extern __shared__ __align__(16) unsigned char stab_smem[];
+    __shared__ __align__(16) StabArgs sa;
+    const int4 tm = b.tiles[blockIdx.x];
+    if (!b.clock[b.inst_clock[tm.x]].active) return;
+    {
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(b.inst + tm.x);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sa);
+        for (int q = threadIdx.x; q < int(sizeof(StabArgs) / 8); q += blockDim.x) dst[q] = src[q];
+    }
+    __syncthreads();
+    stab2d_tile<N>(sa, tm.y, tm.z, stab_smem);
+}
+
 template <int N> __global__ void __launch_bounds__(kThreads) stab1d_kernel(const StabArgs a)
 {
     constexpr int ND = 3 * N;
@@ -412,6 +436,48 @@ template <int N> cudaError_t launch_stab_n(const StabArgs& a, cudaStream_t s)
         stab1d_kernel<N><<<unsigned((lines + kThreads - 1) / kThreads), kThreads, 0, s>>>(a);
     }
     return cudaGetLastError();
+}
+
+template <int N> cudaError_t launch_stab_batch_n(const StabBatchArgs& b, cudaStream_t s)
+{
+    using T = StabTile<N>;
+    auto kern = stab2d_batch_kernel<N>;
+    static bool attr_done[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !attr_done[dev])
+    {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(T::bytes));
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) attr_done[dev] = true;
+    }
+    if (b.ntiles > 0) kern<<<b.ntiles, kThreads, T::bytes, s>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stab_batch(int n, const StabBatchArgs& b, cudaStream_t s)
+{
+    switch (n)
+    {
+        case 2: return launch_stab_batch_n<2>(b, s);
+        case 3: return launch_stab_batch_n<3>(b, s);
+        case 4: return launch_stab_batch_n<4>(b, s);
+        case 5: return launch_stab_batch_n<5>(b, s);
+        case 6: return launch_stab_batch_n<6>(b, s);
+        case 7: return launch_stab_batch_n<7>(b, s);
+        case 8: return launch_stab_batch_n<8>(b, s);
+        case 9: return launch_stab_batch_n<9>(b, s);
+        case 10: return launch_stab_batch_n<10>(b, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+void stab_tile_dims(int n, int* tx, int* ty)
+{
+    const int t = n <= 6 ? 4 : 2;
+    *tx = t;
+    *ty = t;
 }
 
 cudaError_t launch_stab(int n, const StabArgs& a, cudaStream_t s)

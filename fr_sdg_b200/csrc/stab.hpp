@@ -21,6 +21,20 @@ struct StabArgs
 };
 
 cudaError_t launch_stab(int n, const StabArgs& a, cudaStream_t s);
+
+// Post-step of a batch group: every tile of `tiles` is (instance in group, bx, by, -);
+// inst[i] holds instance i's arguments (src = its last stage, dst = its state).
+struct StabBatchArgs
+{
+    const StabArgs*   inst;
+    const int*        inst_clock;  // batch index of each instance (its clock)
+    const BatchClock* clock;
+    const int4*       tiles;
+    int               ntiles;
+};
+cudaError_t launch_stab_batch(int n, const StabBatchArgs& b, cudaStream_t s);
+// tile of the 2D post-step kernel (elements per CTA along x and y)
+void stab_tile_dims(int n, int* tx, int* ty);
 cudaError_t launch_prim_to_cons(int dim, int n, int64_t nelem, const double* in, double* out, cudaStream_t s);
 
 } // namespace frsdg

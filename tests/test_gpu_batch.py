@@ -1,8 +1,6 @@
 """GPU: instances advanced together on a stream pool with graph replays end in the
-same state as each advanced alone and eagerly.  The drawn explosions lose positivity
-in their first steps under the reference's filter-only scheme (the oracle does the
-same), so the comparison starts the drawn meshes and gases from smooth seeded states
-that stay finite."""
+same state as each advanced alone and eagerly, on the drawn meshes and gases from
+smooth seeded states."""
 import pytest
 import torch
 
@@ -27,7 +25,7 @@ def test_batched_matches_standalone(cuda):
             w2 = instance_workload(sp)
             with FRSolver(w2.cfg) as s:
                 V = init(w2.cfg, cuda)
-                Integrator(s, "ssprk3").run(V, cfl_time_step(w2.cfg, V, 0.02), n_steps=12)
+                Integrator(s, "ssprk3").run(V, cfl_time_step(w2.cfg, V, 0.02, w2.cfl_rule), n_steps=12)
                 assert torch.equal(U, V), sp
     finally:
         b.close()
