@@ -291,7 +291,7 @@ def run_reference(args, ws, rank):
     return 0
 
 
-def batched_to_t_end(device, timed, t_end: float = 0.25) -> dict:
+def batched_to_t_end(device, t_end: float = 0.25) -> dict:
     """Config 4 to t_end in FP64 and in the mixed form: time to t_end of all instances
     together, finiteness per instance and the per-instance density L2 of mixed - FP64
     (absolute and relative to the FP64 density's L2 norm)."""
@@ -303,12 +303,13 @@ def batched_to_t_end(device, timed, t_end: float = 0.25) -> dict:
     out, finals = {}, {}
     for mixed in (False, True):
         bi = BatchedInstances(specs, device, mixed=mixed)
-        r, ms = timed(lambda: bi.run(t_end, graph=True))
+        r = bi.run_persistent(t_end)
         finite = [s.status() == 0 and bool(torch.isfinite(U).all()) for _, s, U, _ in bi.items]
         finals[mixed] = [(wl.cfg, U) for wl, _, U, _ in bi.items]
         out["mixed" if mixed else "fp64"] = {
-            "seconds": ms / 1e3, "instances": r.instances, "dofs": r.dofs, "finite_instances": int(sum(finite)),
-            "steps_min_max": [min(r.steps), max(r.steps)], "stage_dof_residuals_per_s": r.stage_residuals / (ms / 1e3)}
+            "seconds": r.seconds, "instances": r.instances, "dofs": r.dofs, "finite_instances": int(sum(finite)),
+            "steps_min_max": [min(r.steps), max(r.steps)], "graph_replays": bi.replays,
+            "stage_dof_residuals_per_s": r.stage_residuals / r.seconds, "tuning": bi.tuning}
         bi.close()
     errs, rels = [], []
     for (cfg, Ud), (_, Um) in zip(finals[False], finals[True]):
@@ -317,7 +318,10 @@ def batched_to_t_end(device, timed, t_end: float = 0.25) -> dict:
         rels.append(e / density_l2(cfg, Ud, torch.zeros_like(Ud)))
     out.update({
         "t_end": t_end, "scheme": "SSP-RK3, spectral filter + positivity limiter on every stage, CFL 0.1 "
-                                  "(dt = CFL h / ((2p+1) c_max)), one CUDA graph of 64 steps per instance, 16 streams",
+                                  "(dt = CFL h / ((2p+1) max(|v|+c)) per instance, re-evaluated on the device "
+                                  "after every step); the batch engine: one launch per order group and stage, "
+                                  "one CUDA graph per step of all instances, device clocks, autotuned tiles "
+                                  "(the autotuner's first pass is inside the timed region)",
         "mixed_vs_fp64_density_l2": {"max": max(errs), "median": statistics.median(errs),
                                      "relative_max": max(rels), "relative_median": statistics.median(rels),
                                      "per_instance": [float(f"{e:.3e}") for e in errs]},
@@ -401,27 +405,35 @@ def run_ours(args, ws, rank, local):
     value = ws * dofs * args.steps / (elapsed_ms / 1e3)
     bad = solver.status()
 
-    # ---- the same residual in FP32 (mixed-precision form), device-resident
+    # ---- the same residual in FP32 (FP32 state), and the RK stage in FP64 and in the
+    # mixed form (FP32 arithmetic on the FP64 state, node primitives recovered in FP64),
+    # device-resident
     mixed = None
     if not args.no_t_end and ws == 1:
         U32 = U.float()
         F32 = torch.empty_like(U32)
-        for _ in range(3):
-            solver.residual_kernel_f32(0.0, U32, F32)
-        barrier()
-        torch.cuda.synchronize()
-        m0 = torch.cuda.Event(enable_timing=True)
-        m1 = torch.cuda.Event(enable_timing=True)
-        m0.record(stream)
-        for _ in range(args.steps):
-            solver.residual_kernel_f32(0.0, U32, F32)
-        m1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-        mms = m0.elapsed_time(m1) / args.steps
+        out = torch.empty_like(U)
+
+        def event_ms(fn):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            m0 = torch.cuda.Event(enable_timing=True)
+            m1 = torch.cuda.Event(enable_timing=True)
+            m0.record(stream)
+            for _ in range(args.steps):
+                fn()
+            m1.record(stream)
+            torch.cuda.synchronize()
+            return m0.elapsed_time(m1) / args.steps
+
+        mms = event_ms(lambda: solver.residual_kernel_f32(0.0, U32, F32))
+        sms = event_ms(lambda: solver.rk_stage(0.0, U, out, gamma=1e-3, a=U, alpha=1.0))
+        xms = event_ms(lambda: solver.rk_stage_mixed(0.0, U, out, gamma=1e-3, a=U, alpha=1.0))
         mixed = {"fp32_residual_ms": mms, "fp32_dof_residuals_per_s": ws * dofs / (mms / 1e3),
-                 "speedup_vs_fp64": (elapsed_ms / args.steps) / mms}
-        del U32, F32
+                 "speedup_vs_fp64": (elapsed_ms / args.steps) / mms,
+                 "fp64_stage_ms": sms, "mixed_stage_ms": xms, "mixed_stage_speedup": sms / xms}
+        del U32, F32, out
 
     # ---- end to end through the host-buffer entry point
     e2e = None
@@ -603,7 +615,7 @@ def run_ours(args, ws, rank, local):
             # with the (2p+1) rule) each marched to t_end = 0.25 with its own time step,
             # in FP64 and in the mixed form (FP32 residuals, FP64 stage sums), with the
             # density L2 difference of the two per instance.
-            batched = batched_to_t_end(f"cuda:{local}", timed)
+            batched = batched_to_t_end(f"cuda:{local}")
             def implicit_figures():
                 # (6) The implicit path on the bump channel (256 x 64, p = 3, 1,048,576 DOF): the
                 # complex-step JVP, the two preconditioner set-ups and applies, and one backward-

@@ -70,7 +70,7 @@ SIGNATURES = {
     "frsdg_jac_blocks": (C.c_int, [_P, _D, _D, _P, _P, _P]),
     "frsdg_residual_f32": (C.c_int, [_P, _D, _P, _P, _P]),
     "frsdg_set_row_window": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
-    "frsdg_rk_stage_mixed": (C.c_int, [_P, _D, _P, _P, _D, _P, _D, _D, _P, _P, _P, _D, _P]),
+    "frsdg_rk_stage_mixed": (C.c_int, [_P, _D, _P, _P, _D, _P, _D, _D, _P, _P, _D, _P]),
     "frsdg_pc_setup": (C.c_int, [_P, _D, _D, _P, _P]),
     "frsdg_pc_apply": (C.c_int, [_P, _P, _P, _P]),
     "frsdg_jac_blocks5": (C.c_int, [_P, _D, _D, _P, _P, _P]),
@@ -83,6 +83,15 @@ SIGNATURES = {
     "frsdg_rhs_host": (C.c_int, [_P, _D, _P, _P, _P]),
     "frsdg_status": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "frsdg_check_state": (C.c_int, [_P, _P, _P]),
+    "frsdg_batch_create": (C.c_int, [C.POINTER(_P), C.c_int32, C.POINTER(_P), C.POINTER(_D), C.POINTER(_D),
+                                     C.POINTER(_D), C.c_int32, C.POINTER(_P)]),
+    "frsdg_batch_step": (C.c_int, [_P, _P]),
+    "frsdg_batch_run": (C.c_int, [_P, C.c_int64, C.POINTER(C.c_int64), _P]),
+    "frsdg_batch_times": (C.c_int, [_P, C.POINTER(_D), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+    "frsdg_batch_groups": (C.c_int, [_P, C.POINTER(C.c_int32)]),
+    "frsdg_batch_tuning": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
+    "frsdg_batch_destroy": (C.c_int, [_P]),
     "frsdg_device_math": (C.c_int, [C.c_int32, _P, _P, C.c_int64, _P]),
     "frsdg_petsc_vec_record_bytes": (C.c_int, [C.c_int64, C.c_int32, C.POINTER(C.c_int64)]),
     "frsdg_petsc_vec_pack": (C.c_int, [_P, C.c_int64, C.c_int32, _P, _P]),

@@ -86,6 +86,74 @@ def instance_workload(spec: InstanceSpec, stab: str = "filter") -> Workload:
     return wl
 
 
+class DeviceBatch:
+    """A batch of instances advanced by the library (frsdg_batch): every SSP-RK3 stage of
+    all instances of a group is one launch, one step of the whole batch is replayed as a
+    CUDA graph until every instance reaches its t_end, and an autotuner picks each
+    group's tile and persistent-CTA count.  items: (FRSolver, state, dt, t_end).
+    dt_scale: per item, adaptive steps dt = dt_scale / max(|v| + c) after every step."""
+
+    def __init__(self, items, mixed: bool = False, dt_scale=None):
+        import ctypes as C
+
+        from . import _abi as A
+
+        self._A, self._C = A, C
+        self.items = list(items)
+        n = len(self.items)
+        hs = (C.c_void_p * n)(*[s._h.value if hasattr(s._h, "value") else s._h for s, _, _, _ in self.items])
+        us = (C.c_void_p * n)(*[U.data_ptr() for _, U, _, _ in self.items])
+        dts = (C.c_double * n)(*[float(dt) for _, _, dt, _ in self.items])
+        tends = (C.c_double * n)(*[float(te) for _, _, _, te in self.items])
+        scales = (C.c_double * n)(*[float(x) for x in dt_scale]) if dt_scale is not None else None
+        self._h = C.c_void_p()
+        A.check(A.lib().frsdg_batch_create(hs, n, us, dts, scales, tends, int(mixed), C.byref(self._h)),
+                "frsdg_batch_create")
+
+    def close(self) -> None:
+        if self._h:
+            self._A.lib().frsdg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self) -> None:
+        self._A.check(self._A.lib().frsdg_batch_step(self._h, torch.cuda.current_stream().cuda_stream),
+                      "frsdg_batch_step")
+
+    def run(self, max_steps: int = 0) -> int:
+        """Replay steps until every instance reaches its t_end (or max_steps > 0 steps)."""
+        C = self._C
+        k = C.c_int64()
+        self._A.check(self._A.lib().frsdg_batch_run(self._h, int(max_steps), C.byref(k),
+                                                    torch.cuda.current_stream().cuda_stream), "frsdg_batch_run")
+        return int(k.value)
+
+    def times(self):
+        """(t, active, steps) of every instance."""
+        C, n = self._C, len(self.items)
+        t, act, st = (C.c_double * n)(), (C.c_int32 * n)(), (C.c_int64 * n)()
+        self._A.check(self._A.lib().frsdg_batch_times(self._h, t, act, st), "frsdg_batch_times")
+        return list(t), [bool(a) for a in act], list(st)
+
+    def tuning(self) -> list[dict]:
+        C = self._C
+        g = C.c_int32()
+        self._A.check(self._A.lib().frsdg_batch_groups(self._h, C.byref(g)), "frsdg_batch_groups")
+        out = []
+        for i in range(g.value):
+            n, var, grid, tiles, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32(), C.c_float()
+            self._A.check(self._A.lib().frsdg_batch_tuning(self._h, i, C.byref(n), C.byref(var), C.byref(grid),
+                                                           C.byref(tiles), C.byref(ms)), "frsdg_batch_tuning")
+            out.append({"order_n": n.value, "tile_variant": var.value, "ctas": grid.value, "tiles": tiles.value,
+                        "stage_ms": ms.value})
+        return out
+
+
 def density_l2(cfg, U: torch.Tensor, V: torch.Tensor) -> float:
     """GLL-quadrature L2 norm of the density difference of two states of one instance
     (physical measure: detJ of the affine map, (h_x/2)(h_y/2))."""
@@ -136,6 +204,40 @@ class BatchedInstances:
         for _, s, _, _ in self.items:
             s.close()
         self.items = []
+
+    def run_persistent(self, t_end: float | None, n_steps: int | None = None, adaptive: bool = True) -> BatchResult:
+        """The whole batch through the library's batch engine (DeviceBatch): one launch per
+        group and stage, one CUDA graph per step replayed until every instance reaches
+        t_end (or for n_steps steps); device-timed, the autotuner's first pass included.
+        adaptive: each instance's step follows its current wave speed (the workload's CFL
+        rule on max |v| + c of the state after every step)."""
+        cur = torch.cuda.current_stream(self.device)
+        for _, s, _, _ in self.items:
+            s.status()
+        dts = [cfl_time_step(wl.cfg, U, wl.cfl, wl.cfl_rule) for wl, _, U, _ in self.items]
+        te = t_end if t_end is not None else float("inf")
+        scales = None
+        if adaptive:
+            scales = []
+            for wl, _, _, _ in self.items:
+                c = wl.cfg
+                h = min(c.box_length[0] / c.n_elems[0], c.box_length[1] / c.n_elems[1])
+                scales.append(wl.cfl * h / ((2 * c.poly_deg + 1) if wl.cfl_rule == "dg" else 1.0))
+        db = DeviceBatch([(s, U, dt, te) for (wl, s, U, it), dt in zip(self.items, dts)], mixed=self.items[0][3].mixed,
+                         dt_scale=scales)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(cur)
+        k = db.run(n_steps or 0)
+        e1.record(cur)
+        torch.cuda.synchronize(self.device)
+        self.times, _, steps = db.times()
+        self.replays = k  # replays of the step graph (inactive instances skip theirs)
+        self.tuning = db.tuning()
+        db.close()
+        finite = sum(1 for _, s, _, _ in self.items if s.status() == 0)
+        stage = float(sum(3 * n * U.numel() for n, (_, _, U, _) in zip(steps, self.items)))
+        return BatchResult(len(self.items), self.dofs, stage, e0.elapsed_time(e1) / 1e3, finite, steps, 0.0)
 
     def run(self, t_end: float | None, cfl: float | None = None, graph: bool = True, n_steps: int | None = None,
             steps_per_graph: int = 64) -> BatchResult:

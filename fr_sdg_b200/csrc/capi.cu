@@ -131,44 +131,6 @@ int report(int code, const char* msg) { return fail(code, msg); }
 int report_cuda(cudaError_t e, const char* what) { return cuda_fail(e, what); }
 } // namespace frsdg
 
-    int          n = 0, Nx = 0, Ny = 0, ndofs = 0;
-    int64_t      ntot = 0, nelem = 0;
-    int          geo = GEO_AFFINE;
-    RefElem      re;
-    Fr2dArgs     a2{};   // template of the 2D launch arguments
-    Fr1dArgs     a1{};
-    StabArgs     st{};
-    double*      d_metrics = nullptr;
-    double*      d_xnorm = nullptr;
-    double*      d_ynorm = nullptr;
-    double*      d_bxy = nullptr;
-    double*      d_detJ = nullptr;   // positivity limiter on curved meshes: detJ per node
-    PPArgs       pp{};               // template of the positivity limiter's launch
-    double*      d_work = nullptr;   // post-step source copy (WENO)
-    double*      d_stage = nullptr;  // host-buffer staging (2 * ntot), allocated on first use
-    unsigned long long* d_bad = nullptr;
-    double*      d_blocks = nullptr;  // preconditioner: element-diagonal Jacobian blocks (FP64)
-    float*       d_inv = nullptr;     // and their inverses (FP32); both allocated by the first frsdg_pc_setup
-    unsigned long long* d_singular = nullptr;
-    double*      d_blocks5 = nullptr; // block Gauss-Seidel: the five blocks of every element row (FP64)
-    float*       d_off = nullptr;     // and the four off-diagonal ones in FP32; allocated by frsdg_pc_setup_gs
-    int          pc_kind = 0;         // 0 none, 1 block Jacobi, 2 block Gauss-Seidel
-    double       jvp_t = 0.0, jvp_sigma = 1.0;
-    const double* jvp_U = nullptr;
-    cudaStream_t last = nullptr;
-    int          device = 0;
-    // row window (frsdg_set_row_window); win_rows == 0: the vectors are the whole mesh
-    int          win_rows = 0, win_base = 0, win_begin = 0, win_end = 0;
-    // frsdg_rhs_host pipeline: upload / compute / download streams and their events
-#ifdef FRSDG_HOST_CHUNKS
-    static constexpr int kHostChunks = FRSDG_HOST_CHUNKS;  // tuning builds
-#else
-    static constexpr int kHostChunks = 32;  // at most; at least 4 element rows per chunk
-#endif
-    cudaStream_t hst[3] = {nullptr, nullptr, nullptr};
-    cudaEvent_t  hev[2 * kHostChunks + 2] = {};
-};
-
 // Element count and vector length of the vectors the entry points see.
 static int64_t local_nelem(const frsdg_handle* h) { return h->win_rows ? int64_t(h->Nx) * h->win_rows : h->nelem; }
 static int64_t local_ntot(const frsdg_handle* h) { return local_nelem(h) * h->ndofs; }
@@ -672,11 +634,13 @@ int frsdg_jvp(frsdg_handle* h, const double* V, double* JV, void* stream)
 
 // Residual pass of the FP32 instantiation (2D): U32 is a float state, out is
 // float (out_f32) or double (the stage forms).
-static int run_residual_f32(frsdg_handle* h, int mode, double t, const float* U32, void* out, bool out_f32,
+// The FP32 instantiation of the 2D kernel; in_f64: U is an FP64 state whose node
+// primitives are recovered in FP64 (the mixed form), else an FP32 state.
+static int run_residual_f32(frsdg_handle* h, int mode, double t, const void* U, bool in_f64, void* out, bool out_f32,
                             const StageArgs* stage, void* stream)
 {
     if (h->cfg.dim != 2) return fail(FRSDG_ERR_UNSUPPORTED, "FP32 residual: 2D configurations only");
-    if ((reinterpret_cast<uintptr_t>(U32) | reinterpret_cast<uintptr_t>(out)) & 15)
+    if ((reinterpret_cast<uintptr_t>(U) | reinterpret_cast<uintptr_t>(out)) & 15)
         return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     h->last = s;
@@ -684,7 +648,8 @@ static int run_residual_f32(frsdg_handle* h, int mode, double t, const float* U3
     a.t = t;
     a.mode = mode;
     a.cond_sys = 0;
-    a.U = reinterpret_cast<const double*>(U32);
+    a.in_f64 = in_f64 ? 1 : 0;
+    a.U = static_cast<const double*>(U);
     a.W = nullptr;
     a.out = out;
     a.out_f32 = out_f32 ? 1 : 0;
@@ -698,17 +663,15 @@ static int run_residual_f32(frsdg_handle* h, int mode, double t, const float* U3
 int frsdg_residual_f32(frsdg_handle* h, double t, const float* U32, float* R32, void* stream)
 {
     if (!h || !U32 || !R32) return fail(FRSDG_ERR_ARG, "null argument");
-    return run_residual_f32(h, MODE_RESIDUAL, t, U32, R32, true, nullptr, stream);
+    return run_residual_f32(h, MODE_RESIDUAL, t, U32, false, R32, true, nullptr, stream);
 }
 
-int frsdg_rk_stage_mixed(frsdg_handle* h, double t, const float* Us32, const double* A, double alpha, const double* B,
-                         double beta, double gamma, double* out, float* out32, double* acc, double delta, void* stream)
+int frsdg_rk_stage_mixed(frsdg_handle* h, double t, const double* Us, const double* A, double alpha, const double* B,
+                         double beta, double gamma, double* out, double* acc, double delta, void* stream)
 {
-    if (!h || !Us32 || !out) return fail(FRSDG_ERR_ARG, "null argument");
-    if (reinterpret_cast<const void*>(out32) == reinterpret_cast<const void*>(Us32))
-        return fail(FRSDG_ERR_ARG, "frsdg_rk_stage_mixed: out32 must not alias Us32");
-    StageArgs st{A, B, acc, alpha, beta, gamma, delta, out32};
-    return run_residual_f32(h, MODE_STAGE, t, Us32, out, false, &st, stream);
+    if (!h || !Us || !out) return fail(FRSDG_ERR_ARG, "null argument");
+    StageArgs st{A, B, acc, alpha, beta, gamma, delta, nullptr};
+    return run_residual_f32(h, MODE_STAGE, t, Us, true, out, false, &st, stream);
 }
 
 int frsdg_set_row_window(frsdg_handle* h, int row_base, int rows, int row_begin, int row_end)

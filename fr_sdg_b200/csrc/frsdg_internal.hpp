@@ -103,6 +103,7 @@ struct Fr2dArgs
     int    exact_bc;   // complex scalars: differentiate the user-lambda boundary kinds too
     int    jac_cmode;  // MODE_JAC colouring: 0 checkerboard, 1 three-colour cycles (odd periodic),
                        // 2 distance-2 colouring (i + 2 j) mod 5 for all five blocks of an element row
+    int    in_f64;     // FP32 instantiation: U is an FP64 state, node primitives recovered in FP64
     Ops    ops;
 };
 
@@ -113,7 +114,13 @@ struct Fr2dArgs
 struct BatchClock
 {
     double t, dt, t_end;
-    int    active, pad_;
+    int    active, adaptive;
+    // adaptive: after every step dt = dt_scale / max(|v| + c) over the instance's
+    // state (amax, the bit pattern of that positive double, gathered by the limiter
+    // pass of the state)
+    double dt_scale;
+    unsigned long long amax;
+    long long steps;   // steps taken
 };
 
 __host__ __device__ inline double batch_step_size(const BatchClock& c)
@@ -129,8 +136,6 @@ struct BatchInst2D
     Fr2dArgs a;
     double*  U;       // state
     double*  b[3];    // SSP-RK3 stage outputs (b[2]: the last, limited into U by the post-step)
-    float*   u32;     // mixed form: FP32 copy of U ...
-    float*   c[2];    // ... and of the first two stage outputs
     int      inst;    // batch index (clock)
     int      pad_;
 };

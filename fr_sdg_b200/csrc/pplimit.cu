@@ -42,6 +42,23 @@ template <int NV> __device__ __forceinline__ double pp_pressure(const PPArgs& a,
     return pp_gas_pressure(a, rho, e);
 }
 
+// |v| + c of a node (the sound speed of the configured gas law, c^2 clamped at 0)
+__device__ __forceinline__ double node_wave_speed(const PPArgs& a, const double* u)
+{
+    const double rho = u[0];
+    const double vx = u[1] / rho, vy = u[2] / rho;
+    const double e = u[3] / rho - 0.5 * (vx * vx + vy * vy);
+    double c2;
+    if (a.gas_law == FRSDG_GAS_IDEAL) c2 = a.gas.gamma * (a.gas.gamma - 1.0) * e;
+    else
+    {
+        const double cov = 1.0 - a.gas.b * rho, gm1 = a.gas.gamma - 1.0;
+        c2 = (a.gas.gamma * gm1 * (e + a.gas.a * rho)) / (cov * cov) +
+             (gm1 * a.gas.a * rho * (2.0 - a.gas.b * rho)) / (cov * cov) - 2.0 * a.gas.a * rho;
+    }
+    return sqrt(vx * vx + vy * vy) + sqrt(fmax(c2, 0.0));
+}
+
 template <int NV>
 __device__ __forceinline__ double pp_segment_root(const PPArgs& a, const double* ub, const double* uq, double eps)
 {
@@ -75,7 +92,7 @@ __device__ __forceinline__ double warp_min(double v)
 // refresh32: write the FP32 copy even when the element is admissible.
 template <int N>
 __device__ __forceinline__ void pp_element2d(const PPArgs& a, double* base, float* base32, int64_t e_glob,
-                                             bool limit, bool refresh32)
+                                             bool limit, bool refresh32, unsigned long long* amax = nullptr)
 {
     constexpr int NQ = N * N, R = (NQ + 31) / 32;
     const int lane = threadIdx.x & 31;
@@ -133,6 +150,16 @@ __device__ __forceinline__ void pp_element2d(const PPArgs& a, double* base, floa
             touched = true;
         }
     }
+    if (amax)
+    {
+        // the largest |v| + c of the (limited) element, for the next adaptive time step
+        double w = 0.0;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (lane + 32 * r < NQ) w = fmax(w, node_wave_speed(a, u[r]));
+        w = -warp_min(-w);
+        if (lane == 0 && w > 0.0 && w < 1e300) atomicMax(amax, static_cast<unsigned long long>(__double_as_longlong(w)));
+    }
     if (!touched && !refresh32) return;
 #pragma unroll
     for (int r = 0; r < R; ++r)
@@ -178,11 +205,13 @@ template <int N> __global__ void __launch_bounds__(256) pp_batch_kernel(const PP
     if (!b.clock[in.inst].active) return;
     const PPArgs& a = b.inst[lo];
     const int64_t e = g - b.elem_begin[lo];
+    // slots 0-2: the stage outputs; 3: the state after the post-step
     double* buf = b.slot == 3 ? in.U : in.b[b.slot];
-    float* buf32 = !b.mixed ? nullptr : b.slot == 3 ? in.u32 : b.slot < 2 ? in.c[b.slot] : nullptr;
-    if (!a.enabled && !(b.slot == 3 && buf32)) return;
-    pp_element2d<N>(a, buf + e * (4 * NQ), buf32 ? buf32 + e * (4 * NQ) : nullptr, 0, a.enabled != 0,
-                    b.slot == 3 && buf32);
+    const bool limit = a.enabled != 0;
+    if (!limit && !(b.slot == 3 && b.clock[in.inst].adaptive)) return;
+    // the state after the post-step also yields the instance's wave speed (adaptive dt)
+    unsigned long long* amax = b.slot == 3 && b.clock[in.inst].adaptive ? &b.clock[in.inst].amax : nullptr;
+    pp_element2d<N>(a, buf + e * (4 * NQ), nullptr, 0, limit, false, amax);
 }
 
 __global__ void batch_clock_kernel(BatchClock* clock, int count, int* active_count)
@@ -195,8 +224,15 @@ __global__ void batch_clock_kernel(BatchClock* clock, int count, int* active_cou
         {
             const double h = batch_step_size(c);
             c.t = h == c.dt ? c.t + c.dt : c.t_end;
+            ++c.steps;
             const double tol = 1e-14 * (c.t_end > 1.0 ? c.t_end : (c.t_end < -1.0 ? -c.t_end : 1.0));
             c.active = c.t < c.t_end - tol;
+            if (c.adaptive)
+            {
+                const double w = __longlong_as_double(static_cast<long long>(c.amax));
+                if (c.amax && w > 0.0) c.dt = c.dt_scale / w;
+                c.amax = 0ull;
+            }
             clock[i] = c;
         }
         if (c.active && active_count) atomicAdd(active_count, 1);

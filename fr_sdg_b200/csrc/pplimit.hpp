@@ -30,9 +30,10 @@ struct PPBatchArgs
     const int64_t*     elem_begin;  // first element of each instance, ninst + 1 entries
     int                ninst;
     int64_t            nelem;
-    const BatchClock*  clock;
-    int                slot;        // 0: b[0] (+c[0]), 1: b[1] (+c[1]), 2: b[2], 3: U (+u32 everywhere when mixed)
-    int                mixed;
+    BatchClock*        clock;       // per batch instance; the limiter pass of the state gathers its
+                                    // max |v| + c into clock[i].amax (adaptive time steps)
+    int                slot;        // 0-2: stage output b[slot]; 3: the state U after the post-step
+    int                pad_;
 };
 cudaError_t launch_pp_batch(int n, const PPBatchArgs& b, cudaStream_t s);
 // advance the clocks of a batch by one step; count the instances still active

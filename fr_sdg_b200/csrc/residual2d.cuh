@@ -202,17 +202,64 @@ template <class S> struct Rec
     S v[RF_N];
 };
 
+// The FP32 instantiation reading an FP64 state (a.in_f64, the mixed form): the node's
+// state is loaded in FP64 and its primitives (density, velocities, internal energy,
+// pressure, and the sound speed when asked) are recovered in FP64 before rounding to
+// FP32, so that pressures near vacuum keep their sign; fluxes, Riemann solves and
+// derivatives then run in FP32.  Returns whether it took that path.
+template <int GAS, class S>
+__device__ __forceinline__ bool node_state_f64(const Fr2dArgs& a, const GasParams& g, int64_t off, S s[4],
+                                               NodePrim<S>& pr, S* c)
+{
+    if constexpr (sizeof(S) == 4)
+    {
+        if (a.in_f64)
+        {
+            double d[4];
+            NodeLoader<double>::load(a, off, d);
+            const NodePrim<double> q = node_prim<GAS>(g, d[0], d[1], d[2], d[3]);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) s[i] = static_cast<float>(d[i]);
+            pr.rho_w = static_cast<float>(q.rho_w);
+            pr.inv_rho = static_cast<float>(q.inv_rho);
+            pr.u = static_cast<float>(q.u);
+            pr.v = static_cast<float>(q.v);
+            pr.e = static_cast<float>(q.e);
+            pr.p = static_cast<float>(q.p);
+            pr.inv_covol = static_cast<float>(q.inv_covol);
+            if (c) *c = static_cast<float>(node_sound_speed<GAS>(g, q));
+            return true;
+        }
+    }
+    return false;
+}
+
 // Boundary ghost record on a physical edge from the interior node's state (rare
 // path, kept out of line; the record returns by value).
 template <int GAS, class S>
 __device__ __noinline__ Rec<S> ghost_record(const Fr2dArgs& a, int dir, int64_t interior_off, double x, double y,
                                             double nx, double ny)
 {
+    Rec<S> out;
+    if constexpr (sizeof(S) == 4)
+    {
+        if (a.in_f64)
+        {
+            double d_in[4], d_out[4];
+            NodeLoader<double>::load(a, interior_off, d_in);
+            bc_ghost2<GAS>(a.bc[dir], dir, a.gas, a.t, x, y, nx, ny, a.Lx, a.Ly, d_in, d_out, false);
+            const NodePrim<double> q = node_prim<GAS>(a.gas, d_out[0], d_out[1], d_out[2], d_out[3]);
+            double r[RF_N];
+            make_record<GAS>(a.gas, d_out, q, r);
+#pragma unroll
+            for (int f = 0; f < RF_N; ++f) out.v[f] = static_cast<float>(r[f]);
+            return out;
+        }
+    }
     S s_in[4], s_out[4];
     NodeLoader<S>::load(a, interior_off, s_in);
     bc_ghost2<GAS>(a.bc[dir], dir, a.gas, a.t, x, y, nx, ny, a.Lx, a.Ly, s_in, s_out, a.exact_bc != 0);
     const NodePrim<S> pr = node_prim<GAS>(a.gas, s_out[0], s_out[1], s_out[2], s_out[3]);
-    Rec<S> out;
     make_record<GAS>(a.gas, s_out, pr, out.v);
     return out;
 }
@@ -409,6 +456,7 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
     static_assert(T::NHALO <= BT, "one halo node per thread");
     S hs[4];
     int hrec = -1;
+    int64_t hoff = 0;
     // the last NHALO threads carry the halo: the first threads may own two tile nodes
     if (tid >= BT - T::NHALO)
     {
@@ -458,7 +506,8 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
         }
         if (ok)
         {
-            NodeLoader<S>::load(a, (int64_t(ge_j) * Nx + ge_i) * ND + node * 4, hs);
+            hoff = (int64_t(ge_j) * Nx + ge_i) * ND + node * 4;
+            if (!(T::F32 && a.in_f64)) NodeLoader<S>::load(a, hoff, hs);
             hrec = r;
         }
     }
@@ -468,15 +517,18 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
         if (tx < txe && ty < tye)
         {
             const int64_t off = (int64_t(j0 + ty) * Nx + (i0 + tx)) * ND + node * 4;
-            S s[4];
-            NodeLoader<S>::load(a, off, s);
+            const bool bnode = k == 0 || k == N - 1 || l == 0 || l == N - 1;
+            S s[4], c64 = S(0.0);
+            NodePrim<S> pr;
+            const bool f64 = node_state_f64<GAS>(a, g, off, s, pr, bnode ? &c64 : nullptr);
+            if (!f64) NodeLoader<S>::load(a, off, s);
             if constexpr (T::JVP)
             {
 #pragma unroll
                 for (int eq = 0; eq < 4; ++eq) sSeed[(e * 4 + eq) * NN + node] = s_im(s[eq]);
             }
             if (!density_ok(s_re(s[0])) && a.bad) atomicAdd(a.bad, 1ull);
-            const NodePrim<S> pr = node_prim<GAS>(g, s[0], s[1], s[2], s[3]);
+            if (!f64) pr = node_prim<GAS>(g, s[0], s[1], s[2], s[3]);
             const S rEp = s[3] + pr.p;
             const S ruv = s[1] * pr.v;
             S* f = sF + e * 4 * NN + node;
@@ -489,10 +541,11 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
             gg[1 * NN] = ruv;
             gg[2 * NN] = s[2] * pr.v + pr.p;
             gg[3 * NN] = pr.v * rEp;
-            if (k == 0 || k == N - 1 || l == 0 || l == N - 1)
+            if (bnode)
             {
                 S rec[RF_N];
                 make_record<GAS>(g, s, pr, rec);
+                if (f64) rec[RF_C] = c64;
                 const int r = e * T::NB + T::bidx(k, l);
 #pragma unroll
                 for (int fld = 0; fld < RF_N; ++fld) sRec[fld * NREC + r] = rec[fld];
@@ -501,9 +554,13 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
     }
     if (hrec >= 0)
     {
-        const NodePrim<S> pr = node_prim<GAS>(g, hs[0], hs[1], hs[2], hs[3]);
+        NodePrim<S> pr;
+        S c64 = S(0.0);
+        const bool f64 = node_state_f64<GAS>(a, g, hoff, hs, pr, &c64);
+        if (!f64) pr = node_prim<GAS>(g, hs[0], hs[1], hs[2], hs[3]);
         S rec[RF_N];
         make_record<GAS>(g, hs, pr, rec);
+        if (f64) rec[RF_C] = c64;
 #pragma unroll
         for (int fld = 0; fld < RF_N; ++fld) sRec[fld * NREC + hrec] = rec[fld];
     }
@@ -730,7 +787,9 @@ cudaError_t launch_fr2d_kernel(const Fr2dArgs& a, cudaStream_t st)
 // Stage k of SSP-RK3 (Shu and Osher) for instance `in` at its own clock, in the form the
 // integrator's stages take (fr_sdg_b200/integrate.py):
 //   k = 0: b0 = U + h L(U);  k = 1: b1 = 3/4 U + 1/4 b0 + h/4 L(b0);
-//   k = 2: b2 = 1/3 U + 2/3 b1 + 2h/3 L(b1);  the mixed form reads the FP32 copies.
+//   k = 2: b2 = 1/3 U + 2/3 b1 + 2h/3 L(b1).
+// The mixed form (FP32 instantiation) reads the same FP64 stage inputs and recovers
+// every node's primitives in FP64 (Fr2dArgs::in_f64).
 __device__ __forceinline__ void batch_stage_args(Fr2dArgs& a, const BatchInst2D& in, const BatchClock& ck, int k,
                                                  bool mixed)
 {
@@ -738,41 +797,40 @@ __device__ __forceinline__ void batch_stage_args(Fr2dArgs& a, const BatchInst2D&
     a.mode = MODE_STAGE;
     a.cond_sys = 0;
     a.out_f32 = 0;
+    a.in_f64 = mixed ? 1 : 0;
     a.W = nullptr;
     a.st.acc = nullptr;
     a.st.delta = 0.0;
+    a.st.out32 = nullptr;
     a.st.A = in.U;
     if (k == 0)
     {
-        a.U = mixed ? reinterpret_cast<const double*>(in.u32) : in.U;
+        a.U = in.U;
         a.out = in.b[0];
         a.st.B = nullptr;
         a.st.alpha = 1.0;
         a.st.beta = 0.0;
         a.st.gamma = h;
-        a.st.out32 = mixed ? in.c[0] : nullptr;
         a.t = ck.t;
     }
     else if (k == 1)
     {
-        a.U = mixed ? reinterpret_cast<const double*>(in.c[0]) : in.b[0];
+        a.U = in.b[0];
         a.out = in.b[1];
         a.st.B = in.b[0];
         a.st.alpha = 0.75;
         a.st.beta = 0.25;
         a.st.gamma = 0.25 * h;
-        a.st.out32 = mixed ? in.c[1] : nullptr;
         a.t = ck.t + h;
     }
     else
     {
-        a.U = mixed ? reinterpret_cast<const double*>(in.c[1]) : in.b[1];
+        a.U = in.b[1];
         a.out = in.b[2];
         a.st.B = in.b[1];
         a.st.alpha = 1.0 / 3.0;
         a.st.beta = 2.0 / 3.0;
         a.st.gamma = 2.0 * h / 3.0;
-        a.st.out32 = nullptr;
         a.t = ck.t + 0.5 * h;
     }
 }

@@ -78,9 +78,9 @@ class RunStats:
 class Integrator:
     """SSP-RK3 / RK4 over one FRSolver; buffers are allocated once.
 
-    mixed=True: every stage takes the residual in FP32 from an FP32 copy of its input
-    (frsdg_rk_stage_mixed) and combines the stages in FP64; the FP64 state stays the
-    solution.  The FP32 copy of U is refreshed at the end of every step."""
+    mixed=True: every stage takes the residual in FP32 arithmetic from its FP64 input,
+    whose node primitives are recovered in FP64 (frsdg_rk_stage_mixed), and combines
+    the stages in FP64; the FP64 state stays the solution."""
 
     def __init__(self, solver: FRSolver, scheme: str = "ssprk3", mixed: bool = False, before_stage=None):
         """before_stage(V): called with every stage input and with U before the post-step
@@ -93,8 +93,6 @@ class Integrator:
         self.scheme = scheme
         self.mixed = mixed
         self.before = before_stage
-        if mixed and before_stage is not None:
-            raise ValueError("before_stage: FP64 stages only")
         self._buf = None
         cfg = solver.cfg
         self.stabilise = bool(cfg.apply_filter or cfg.apply_weno)
@@ -105,44 +103,20 @@ class Integrator:
     def _buffers(self, U: torch.Tensor):
         if self._buf is None or self._buf[0].device != U.device:
             self._buf = [torch.empty_like(U) for _ in range(3)]
-            if self.mixed:
-                self._buf += [torch.empty(U.shape, dtype=torch.float32, device=U.device) for _ in range(3)]
         return self._buf
-
-    def _step_mixed(self, U: torch.Tensor, t: float, dt: float) -> None:
-        s = self.s
-        b1, b2, b3, u32, c1, c2 = self._buffers(U)
-        u32.copy_(U)
-
-        def stage(tt, us32, out, out32, **kw):
-            s.rk_stage_mixed(tt, us32, out, out32, **kw)
-            if self.pp:
-                s.pp_limit(out, out32)
-
-        if self.scheme == "ssprk3":
-            stage(t, u32, b1, c1, gamma=dt, a=U, alpha=1.0)
-            stage(t + dt, c1, b2, c2, gamma=0.25 * dt, a=U, alpha=0.75, b=b1, beta=0.25)
-            stage(t + 0.5 * dt, c2, U, None, gamma=2.0 * dt / 3.0, a=U, alpha=1.0 / 3.0, b=b2, beta=2.0 / 3.0)
-        else:
-            b3.copy_(U)
-            stage(t, u32, b1, c1, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 6.0)
-            stage(t + 0.5 * dt, c1, b2, c2, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
-            stage(t + 0.5 * dt, c2, b1, c1, gamma=dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
-            stage(t + dt, c1, U, None, gamma=dt / 6.0, a=b3, alpha=1.0)
-        if self.stabilise:
-            s.apply_stabilization(U)
 
     def _rk(self, t: float, Us: torch.Tensor, out: torch.Tensor, **kw) -> None:
         if self.before is not None:
             self.before(Us)
-        self.s.rk_stage(t, Us, out, **kw)
+        if self.mixed:
+            self.s.rk_stage_mixed(t, Us, out, **kw)
+        else:
+            self.s.rk_stage(t, Us, out, **kw)
         if self.pp:
             self.s.pp_limit(out)
 
     def step(self, U: torch.Tensor, t: float, dt: float) -> None:
         """Advance U (in place) from t to t + dt, then apply the post-step limiter."""
-        if self.mixed:
-            return self._step_mixed(U, t, dt)
         s = self.s
         b1, b2, b3 = self._buffers(U)[:3]
         # with a limiter, the last stage goes to a free buffer and the limiter writes U

@@ -104,15 +104,15 @@ class FRSolver:
         self._check_f32(U32, R32)
         A.check(self._lib.frsdg_residual_f32(self._h, t, _ptr(U32), _ptr(R32), _stream()), "frsdg_residual_f32")
 
-    def rk_stage_mixed(self, t: float, Us32: torch.Tensor, out: torch.Tensor, out32: torch.Tensor | None,
-                       gamma: float, a: torch.Tensor | None = None, alpha: float = 0.0, b: torch.Tensor | None = None,
+    def rk_stage_mixed(self, t: float, Us: torch.Tensor, out: torch.Tensor, gamma: float,
+                       a: torch.Tensor | None = None, alpha: float = 0.0, b: torch.Tensor | None = None,
                        beta: float = 0.0, acc: torch.Tensor | None = None, delta: float = 0.0) -> None:
-        """out = alpha a + beta b + gamma rhs32(Us32) in FP64, out32 = float(out); acc += delta rhs."""
-        self._check_f32(Us32, *(v for v in (out32,) if v is not None))
-        self._check_vec(out, *(v for v in (a, b, acc) if v is not None))
+        """out = alpha a + beta b + gamma rhs32(Us) in FP64, acc += delta rhs: the residual
+        in FP32 arithmetic from the FP64 state Us, node primitives recovered in FP64."""
+        self._check_vec(Us, out, *(v for v in (a, b, acc) if v is not None))
         p = lambda v: _ptr(v) if v is not None else None
-        A.check(self._lib.frsdg_rk_stage_mixed(self._h, t, _ptr(Us32), p(a), alpha, p(b), beta, gamma, _ptr(out),
-                                               p(out32), p(acc), delta, _stream()), "frsdg_rk_stage_mixed")
+        A.check(self._lib.frsdg_rk_stage_mixed(self._h, t, _ptr(Us), p(a), alpha, p(b), beta, gamma, _ptr(out),
+                                               p(acc), delta, _stream()), "frsdg_rk_stage_mixed")
 
     def pre_jv_eval(self, t: float, U: torch.Tensor, sigma: float) -> None:
         self._check_vec(U)

@@ -194,14 +194,17 @@ int frsdg_set_row_window(frsdg_handle* h, int row_base, int rows, int row_begin,
 
 /* Mixed precision (2D; no reference counterpart -- the reference computes in FP64
  * only).  frsdg_residual_f32: R = residual_kernel evaluated in FP32 on an FP32 state.
- * frsdg_rk_stage_mixed: frsdg_rk_stage with the residual taken in FP32 from Us32 and the
- * stage combination in FP64:
- *   out = alpha*A + beta*B + gamma*rhs(Us32),  out32 = (float)out,  acc += delta*rhs
- * (A, B, acc, out32 may be NULL; out32 must not alias Us32).  No change of variables. */
+ * frsdg_rk_stage_mixed: frsdg_rk_stage on the FP64 stage input Us with the residual in
+ * FP32 arithmetic: every node's density, velocities, internal energy, pressure and sound
+ * speed are recovered from the FP64 state in FP64 (so that pressures near vacuum keep
+ * their sign) and rounded to FP32; fluxes, Riemann solves and derivative contractions
+ * run in FP32; the stage combination is FP64:
+ *   out = alpha*A + beta*B + gamma*rhs(Us),  acc += delta*rhs
+ * (A, B, acc may be NULL).  No change of variables. */
 int frsdg_residual_f32(frsdg_handle* h, double t, const float* U32, float* R32, void* stream);
-int frsdg_rk_stage_mixed(frsdg_handle* h, double t, const float* Us32, const double* A, double alpha,
-                         const double* B, double beta, double gamma, double* out, float* out32,
-                         double* acc, double delta, void* stream);
+int frsdg_rk_stage_mixed(frsdg_handle* h, double t, const double* Us, const double* A, double alpha,
+                         const double* B, double beta, double gamma, double* out, double* acc,
+                         double delta, void* stream);
 
 /* Element-diagonal blocks of the implicit Jacobian J = sigma*dM/dU + dR(M(U))/dU at
  * (t, U), by complex step (h = cfg.csd_eps) with element colouring, in one launch:
@@ -266,8 +269,8 @@ int frsdg_post_step_to(frsdg_handle* h, const double* src, double* dst, void* st
  * per element, scale the density about its cell average until rho >= eps, then the
  * whole state until p >= eps (Zhang and Shu, J. Comput. Phys. 229 (2010) 8918-8934),
  * eps = min(cfg.pp_eps, rho_bar, p_bar); elements already admissible are left
- * untouched.  U32 (2D, may be NULL): an FP32 copy of U refreshed where U changes (the
- * mixed-precision stage input).  Does nothing unless cfg.pp_limit.  frsdg_post_step and
+ * untouched.  U32 (2D, may be NULL): an FP32 copy of U refreshed where U changes (for
+ * callers that keep one for frsdg_residual_f32).  Does nothing unless cfg.pp_limit.  frsdg_post_step and
  * frsdg_post_step_to apply it after the stabilisation themselves; a time integrator
  * calls it on the output of every Runge-Kutta stage. */
 int frsdg_pp_limit(frsdg_handle* h, double* U, float* U32, void* stream);
@@ -286,6 +289,47 @@ int frsdg_rhs_host(frsdg_handle* h, double t, const double* U_host, double* rhs_
  * (0 = healthy); the count restarts at zero.  Synchronises the handle's last
  * stream. */
 int frsdg_status(frsdg_handle* h, int64_t* bad_nodes);
+
+/* ---- batches of independent instances (no counterpart in the reference, which
+ * runs one problem per process) -------------------------------------------------
+ * A batch advances `count` 2D instances -- handles on the current device with affine
+ * geometry, no row window and no change of variables -- by SSP-RK3 from t = 0 to their
+ * own t_end with their own time step dt (the last step clipped to land on t_end, like
+ * TS_EXACTFINALTIME_MATCHSTEP, petsc_solver_impl.hpp:556), each followed by its
+ * handle's post-step (stabilisation and positivity limiter; the limiter also acts on
+ * every stage output when cfg.pp_limit).  states[i] is instance i's device state,
+ * advanced in place; the handles and states must outlive the batch.  mixed = 1: the
+ * stages of frsdg_rk_stage_mixed (FP32 residual arithmetic, node primitives recovered
+ * from the FP64 stage inputs in FP64, stage sums in FP64).
+ * Instances sharing order, gas law, flux and VCJH correction form a group; one step is
+ * one residual-and-stage launch per group and stage over the concatenated tiles of the
+ * group's instances, one limiter launch per group and stage, one post-step launch per
+ * group and one clock update: no host work per instance.  The first step or run times
+ * the candidate tiles and persistent-CTA counts of every group with CUDA events and
+ * keeps the fastest (cached per device, order, gas law, flux, precision and size).
+ * frsdg_batch_step enqueues one step; frsdg_batch_run captures one step into a CUDA graph
+ * and replays it until every instance has reached t_end (or max_steps > 0 steps),
+ * reading the device's count of active instances every 16 steps, and returns the
+ * number of steps taken.  Each handle's health word counts its instance's bad nodes.
+ * dt_scale (may be NULL: fixed steps dt[i]): adaptive steps -- after every step,
+ * dt = dt_scale[i] / max(|v| + c) over the instance's state (a CFL number times the
+ * element size), which keeps the positivity limiter's CFL bound when near-vacuum nodes
+ * raise the wave speed; dt[i] is the first step. */
+typedef struct frsdg_batch frsdg_batch;
+int frsdg_batch_create(frsdg_handle* const* handles, int32_t count, double* const* states, const double* dt,
+                       const double* dt_scale, const double* t_end, int32_t mixed, frsdg_batch** out);
+int frsdg_batch_step(frsdg_batch* b, void* stream);
+int frsdg_batch_run(frsdg_batch* b, int64_t max_steps, int64_t* steps, void* stream);
+/* current time of every instance (t[count]), whether it is still active and the steps it
+ * has taken (active, steps: may be NULL) */
+int frsdg_batch_times(const frsdg_batch* b, double* t, int32_t* active, int64_t* steps);
+/* number of groups, and the autotuner's choice for one: order n, tile variant (0: the
+ * tuned shape, 1: half its element rows), persistent CTAs of the stage launch, tiles,
+ * and the stage launch time that decided it (ms) */
+int frsdg_batch_groups(const frsdg_batch* b, int32_t* groups);
+int frsdg_batch_tuning(const frsdg_batch* b, int32_t group, int32_t* order, int32_t* variant, int32_t* grid,
+                       int32_t* tiles, float* stage_ms);
+int frsdg_batch_destroy(frsdg_batch* b);
 
 /* Add to the health word the nodes of U whose density is not positive and finite
  * (read back by frsdg_status).  The residual calls count the states they read; this
