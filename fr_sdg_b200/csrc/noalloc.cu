@@ -15,6 +15,8 @@
 #include "stab.hpp"
 
 #include <cmath>
+#include <mutex>
+#include <vector>
 
 namespace frsdg
 {
@@ -33,25 +35,65 @@ namespace
 // overwrites the part it reads before reading it, so nothing needs clearing.
 static __device__ __align__(256) double g_post_step_scratch[FRSDG_POST_STEP_STATIC_MAX_DOFS];
 
-constexpr int kMaxDevices = 64;
-double* g_scratch_ptr[kMaxDevices] = {};
+// Device address of the scratch array in the calling thread's current CUDA context.
+// The host-side name of a __device__ array is not a device address, and the address
+// belongs to the context (a device reset makes a new one), so the lookups are cached
+// per context, under a mutex: host threads may call concurrently.
+using CtxGetCurrent = int (*)(void**);  // cuCtxGetCurrent, through the runtime's entry points
 
-// Device address of the scratch array on the current device, looked up once per
-// device (the host-side name of a __device__ array is not a device address).
+void* current_context()
+{
+    static CtxGetCurrent fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetCurrent>(f);
+    }();
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
+
+struct ScratchEntry
+{
+    void*   ctx;
+    double* ptr;
+};
+std::mutex g_scratch_mu;
+std::vector<ScratchEntry> g_scratch;
+
 int scratch_address(double** out)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return report_cuda(e, "cudaGetDevice");
-    if (dev < 0 || dev >= kMaxDevices) return report(FRSDG_ERR_UNSUPPORTED, "device ordinal above 63");
-    if (!g_scratch_ptr[dev])
+    void* ctx = current_context();
     {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_post_step_scratch);
-        if (e != cudaSuccess) return report_cuda(e, "cudaGetSymbolAddress(post-step scratch)");
-        g_scratch_ptr[dev] = static_cast<double*>(p);
+        std::lock_guard<std::mutex> lk(g_scratch_mu);
+        for (const ScratchEntry& e : g_scratch)
+            if (ctx && e.ctx == ctx)
+            {
+                *out = e.ptr;
+                return FRSDG_OK;
+            }
     }
-    *out = g_scratch_ptr[dev];
+    // first call in this context (or no context yet: the lookup creates the primary one)
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_post_step_scratch);
+    if (e != cudaSuccess) return report_cuda(e, "cudaGetSymbolAddress(post-step scratch)");
+    ctx = current_context();
+    if (ctx)
+    {
+        std::lock_guard<std::mutex> lk(g_scratch_mu);
+        bool seen = false;
+        for (ScratchEntry& x : g_scratch)
+            if (x.ctx == ctx)
+            {
+                x.ptr = static_cast<double*>(p);
+                seen = true;
+            }
+        if (!seen) g_scratch.push_back({ctx, static_cast<double*>(p)});
+    }
+    *out = static_cast<double*>(p);
     return FRSDG_OK;
 }
 } // namespace

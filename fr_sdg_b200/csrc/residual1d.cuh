@@ -30,7 +30,7 @@ template <> struct NodeLoader1D<cplx>
     }
 };
 
-// prim_to_cons_elem (problem_def.hpp:286-301) for one 1D node in place.
+// prim_to_cons_elem (problem_def.hpp:36-51) for one 1D node in place.
 template <class S> __device__ __forceinline__ void prim_to_cons1(S s[3])
 {
     const S rho  = s_exp(s[0]);

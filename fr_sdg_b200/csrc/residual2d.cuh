@@ -121,7 +121,7 @@ template <> struct NodeLoader<double>
         s[0] = x0.x; s[1] = x0.y; s[2] = x1.x; s[3] = x1.y;
         if (a.cond_sys)
         {
-            // prim_to_cons_elem (problem_def.hpp:286-301)
+            // prim_to_cons_elem (problem_def.hpp:36-51)
             const double rho  = exp(s[0]);
             const double ssq  = (0.0 + s[1] * s[1]) + s[2] * s[2];
             const double rhoE = rho * (exp(s[3]) + 0.5 * ssq);

@@ -5,7 +5,7 @@
 // for exact symmetry (D. A. Kopriva, "Implementing Spectral Methods for PDEs",
 // Springer 2009, Algorithm 25).  Weights 2 / (p (p+1) P_p(x)^2) as in
 // reference_element.hpp:104-115.  Differentiation matrix and VCJH correction
-// derivatives follow cached_computations.hpp:237-334 (Vincent, Castonguay and
+// derivatives follow cached_computations.hpp:37-137 (Vincent, Castonguay and
 // Jameson, J. Sci. Comput. 47, 2011).  The filter's inverse Vandermonde matrix
 // is the discrete Legendre transform on the GLL points (exact for this node
 // set), in place of the reference's LU inverse (filter.hpp:451-484).

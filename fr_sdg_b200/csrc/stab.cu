@@ -381,7 +381,7 @@ template <int N> __global__ void __launch_bounds__(kThreads) stab1d_kernel(const
     for (int t = 0; t < N; ++t) a.dst[int64_t(e) * ND + eq * N + t] = o[t];
 }
 
-// prim_to_cons_elem (problem_def.hpp:286-301) on every node.
+// prim_to_cons_elem (problem_def.hpp:36-51) on every node.
 __global__ void prim_to_cons2d_kernel(const double* __restrict__ in, double* __restrict__ out, int64_t nodes)
 {
     const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;

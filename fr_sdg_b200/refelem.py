@@ -12,7 +12,7 @@ from . import _abi as A
 @lru_cache(maxsize=None)
 def reference_element(p: int, radau_corr: float = 0.0):
     """(nodes, weights, D, dL, dR) of degree p: GLL (reference_element.hpp:50-147) and
-    CachedElementData (cached_computations.hpp:225-334) as built by the library."""
+    CachedElementData (cached_computations.hpp:8-137) as built by the library."""
     n = p + 1
     x, w, dl, dr = (np.zeros(n) for _ in range(4))
     D = np.zeros((n, n))

@@ -113,7 +113,7 @@ def node_coords(cfg: A.frsdg_config, device="cpu", rows: tuple[int, int] | None 
 
 
 def rhoE(gas: str, gamma: float, a: float, b: float, rho, vel2, p):
-    """get_rhoE of the gas laws (gas_models.hpp:241-246, 304-317) with |v|^2 given."""
+    """get_rhoE of the gas laws (gas_models.hpp:81-86, 144-157) with |v|^2 given."""
     if gas == "ideal":
         return p / (gamma - 1.0) + 0.5 * rho * vel2
     a_rho_sq = a * rho * rho

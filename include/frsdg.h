@@ -354,10 +354,15 @@ int frsdg_device_math(int32_t op, const double* x, double* y, int64_t n, void* s
  * counterpart in the reference.  It takes the configuration instead of a handle
  * and allocates nothing: the copy the WENO limiter reads from is a fixed device
  * array of FRSDG_POST_STEP_STATIC_MAX_DOFS doubles inside the library; larger
- * solutions are rejected with FRSDG_ERR_ARG.  The first call on each device looks
- * up that array's device address, so make the first call outside any stream
+ * solutions are rejected with FRSDG_ERR_ARG.  The first call in each CUDA context
+ * looks up that array's device address, so make the first call outside any stream
  * capture.  Calls share the array: calls that overlap on the GPU (different
  * streams, or different host threads) race and must be ordered by the caller.
+ * Every call rebuilds the small operators (filter matrix, differentiation matrix,
+ * GLL weights) on the host from the configuration -- a few microseconds of host work
+ * per call for p <= 9 -- and passes them by value to the kernel; a caller that
+ * limits the same configuration often and may allocate should keep a handle and
+ * call frsdg_post_step instead.
  * Results equal frsdg_post_step's for the same configuration and input. */
 int frsdg_post_step_static(const frsdg_config* cfg, double* U, void* stream);
 
@@ -378,7 +383,7 @@ int frsdg_petsc_vec_pack(const double* x, int64_t n, int32_t index_bytes, void* 
 
 /* Host-only set-up operators, usable without a GPU.
  * Reference element: GLL (reference_element.hpp:50-147) and CachedElementData
- * (cached_computations.hpp:225-334).  Arrays: nodes[n], weights[n], D[n*n]
+ * (cached_computations.hpp:8-137).  Arrays: nodes[n], weights[n], D[n*n]
  * (row-major D(i,j)), dL[n], dR[n] with n = p+1. */
 int frsdg_reference_element(int32_t p, double radau_corr, double* nodes, double* weights,
                             double* D, double* dL, double* dR);

@@ -10,7 +10,7 @@
 //   include/gas_models.hpp:56-158              IdealGas, VanDerWaals
 //   include/riemann_solver.hpp:20-349          make_state, fluxes, Rusanov/HLLC 1D and 2D
 //   include/reference_element.hpp:50-147       GLL nodes (Golub-Welsch) and weights
-//   include/cached_computations.hpp:237-334    VCJH dL/dR, differentiation matrix
+//   include/cached_computations.hpp:37-137     VCJH dL/dR, differentiation matrix
 //   include/filter.hpp:397-755                 spectral filter, WENO, shock sensor
 //   include/geometry_models.hpp:72-195         Cartesian and de Laval geometry policies
 //   tests/bump.cpp:13-171, tests/boundary_conforming.cpp:14-120  wall-profile geometries
@@ -18,7 +18,7 @@
 //   include/physics_evaluator.hpp:234-313      computational coordinates, composite metrics
 //   include/physics_impl_2D.hpp:76-124, 126-154, 268-357, 646-902
 //   include/physics_impl_1D.hpp:9-94, 96-121, 124-181, 183-205
-//   include/problem_def.hpp:286-320            prim <-> cons change of variables
+//   include/problem_def.hpp:36-70              prim <-> cons change of variables
 //   include/petsc_solver_impl.hpp:250-432, 626-670, 683-702  JVP, IFunction, RHS, post step
 //
 // The reference cannot be compiled here (it needs PETSc, MPI, Eigen, Boost.Math and a
@@ -368,7 +368,7 @@ struct RefElement
     std::vector<double> csi, w, D, dL, dR; // D row-major n*n
 };
 
-// reference_element.hpp:50-147 and cached_computations.hpp:225-334
+// reference_element.hpp:50-147 and cached_computations.hpp:8-137
 inline RefElement make_ref_element(int p, double c_rad)
 {
     if (p < 1 || p > 9) throw std::invalid_argument("poly_deg must be in [1, 9]");
@@ -414,7 +414,7 @@ inline RefElement make_ref_element(int p, double c_rad)
         r.csi = {-1.0, 1.0};
         r.w   = {1.0, 1.0};
     }
-    // create_diff_matrix (cached_computations.hpp:303-334)
+    // create_diff_matrix (cached_computations.hpp:107-137)
     r.D.assign(n * n, 0.0);
     std::vector<double> a(n, 1.0);
     for (int i = 0; i < n; ++i)
@@ -433,7 +433,7 @@ inline RefElement make_ref_element(int p, double c_rad)
                 r.D[i * n + i] = s;
             }
         }
-    // build_Radaus_poly_deriv (cached_computations.hpp:237-280)
+    // build_Radaus_poly_deriv (cached_computations.hpp:37-105)
     r.dL.assign(n, 0.0);
     r.dR.assign(n, 0.0);
     const double sign = (p % 2 == 0) ? 1.0 : -1.0;
@@ -1130,7 +1130,7 @@ template <class U> void residual(const Problem& P, double t, const U* X, U* R)
 }
 
 // ---------------------------------------------------------------- change of variables
-// problem_def.hpp:286-301, called per node as in physics_impl_2D.hpp:126-154 and
+// problem_def.hpp:36-51, called per node as in physics_impl_2D.hpp:126-154 and
 // physics_impl_1D.hpp:183-205.
 template <class U> void prim_to_cons(const Problem& P, const U* prim, U* cons)
 {

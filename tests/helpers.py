@@ -67,7 +67,7 @@ def random_state(cfg, seed: int, amp: float = 0.4, smooth: bool = False) -> np.n
 
 
 def cons_to_prim(cfg, U: np.ndarray) -> np.ndarray:
-    """(log rho, u, [v], log e) of a conservative vector (problem_def.hpp:306-320)."""
+    """(log rho, u, [v], log e) of a conservative vector (problem_def.hpp:56-70)."""
     n = cfg.poly_deg + 1
     if cfg.dim == 2:
         q = U.reshape(-1, 4)

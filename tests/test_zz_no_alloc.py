@@ -60,3 +60,36 @@ def test_static_post_step_rejects_oversize(cuda):
     rc = A.lib().frsdg_post_step_static(C.byref(cfg), U.data_ptr(), None)
     assert rc == A.ERR_ARG
     assert b"FRSDG_POST_STEP_STATIC_MAX_DOFS" in A.lib().frsdg_last_error()
+
+
+@pytest.mark.parametrize("dim", [2, 1])
+def test_static_post_step_replays_in_a_cuda_graph(dim, cuda):
+    """The use the entry point exists for: after one warm-up call outside capture, the
+    WENO post-step is captured into a CUDA graph (no allocation is allowed there) and
+    every replay limits the graph's input buffer exactly as frsdg_post_step does."""
+    if dim == 2:
+        cfg = make_config(dim=2, p=3, n_elems=(8, 6), box=(1.0, 1.0), riemann="hllc",
+                          bcs={A.LEFT: A.BC_PERIODIC, A.RIGHT: A.BC_PERIODIC, A.TOP: A.BC_WALL,
+                               A.BOTTOM: A.BC_OUTFLOW})
+    else:
+        cfg = make_config(dim=1, p=4, n_elems=(32, 1), riemann="rusanov",
+                          bcs={A.LEFT: A.BC_OUTFLOW, A.RIGHT: A.BC_OUTFLOW})
+    cfg.apply_weno = 1
+    cfg.shock_threshold = 0.3
+    buf = torch.from_numpy(random_state(cfg, seed=40)).to(cuda)
+    _static(cfg, buf.clone())  # warm-up: the scratch address is looked up outside capture
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        _static(cfg, buf)
+    for seed in (41, 42):
+        U0 = torch.from_numpy(random_state(cfg, seed=seed)).to(cuda)
+        buf.copy_(U0)
+        g.replay()
+        ref = U0.clone()
+        with FRSolver(cfg) as s:
+            s.apply_stabilization(ref)
+        torch.cuda.synchronize()
+        err = rel_err(buf.cpu().numpy(), ref.cpu().numpy())
+        assert err <= TOL_FP64, f"{dim}D seed {seed}: rel err {err:.3e}"
+    del g
