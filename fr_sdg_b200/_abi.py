@@ -13,6 +13,8 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libfrsdg.so"
 
 POST_STEP_STATIC_MAX_DOFS = 4194304  # FRSDG_POST_STEP_STATIC_MAX_DOFS in include/frsdg.h
+# frsdg_rk_stage_fused flags
+STAGE_MIXED, STAGE_LIMIT, STAGE_POST_STEP = 1, 2, 4
 
 # status codes
 OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NODEVICE = 0, -1, -2, -3, -4, -5
@@ -71,6 +73,7 @@ SIGNATURES = {
     "frsdg_residual_f32": (C.c_int, [_P, _D, _P, _P, _P]),
     "frsdg_set_row_window": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
     "frsdg_rk_stage_mixed": (C.c_int, [_P, _D, _P, _P, _D, _P, _D, _D, _P, _P, _D, _P]),
+    "frsdg_rk_stage_fused": (C.c_int, [_P, _D, _P, _P, _D, _P, _D, _D, _P, _P, _D, C.c_int32, _P]),
     "frsdg_pc_setup": (C.c_int, [_P, _D, _D, _P, _P]),
     "frsdg_pc_apply": (C.c_int, [_P, _P, _P, _P]),
     "frsdg_jac_blocks5": (C.c_int, [_P, _D, _D, _P, _P, _P]),

@@ -95,7 +95,8 @@ struct Group
     StabArgs* d_stab = nullptr;
     int*   d_stab_clock = nullptr;
     int4*  d_stab_tiles = nullptr;
-    int    nstab = 0;
+    int    nstab = 0;              // post-step tiles of the instances whose post-step is not fused
+    int    unfused = 0;            // such instances
     PPArgs* d_pp = nullptr;
     int64_t* d_elem_begin = nullptr;
     int64_t nelem = 0;
@@ -112,6 +113,7 @@ struct frsdg_batch
     std::vector<frsdg_handle*> handles;
     std::vector<Group> groups;
     BatchClock* d_clock = nullptr;
+    PostArgs* d_post = nullptr;  // stage-epilogue operands per instance
     int*   d_active = nullptr;
     int*   h_active = nullptr;  // pinned
     std::vector<void*> allocs;
@@ -141,6 +143,7 @@ void free_batch(frsdg_batch* b)
     }
     for (void* p : b->allocs) cudaFree(p);
     cudaFree(b->d_clock);
+    cudaFree(b->d_post);
     cudaFree(b->d_active);
     if (b->h_active) cudaFreeHost(b->h_active);
     for (cudaEvent_t& e : b->ev)
@@ -189,24 +192,25 @@ cudaError_t launch_pp(const frsdg_batch* b, const Group& g, int slot, cudaStream
     return launch_pp_batch(g.n, p, s);
 }
 
-// One SSP-RK3 step of every active instance, enqueued on s.
+// One SSP-RK3 step of every active instance, enqueued on s.  Every stage launch limits
+// its outputs in its epilogue; for instances with an element-local post-step (the
+// filter, the limiter) the last stage's epilogue is the whole post-step and writes the
+// state, so a group of such instances takes three launches per step.  The WENO
+// post-step of the others follows as its own pass, then their limiter and wave speeds.
 cudaError_t enqueue_step(const frsdg_batch* b, cudaStream_t s)
 {
     cudaError_t e;
     for (int k = 0; k < 3; ++k)
-    {
         for (const Group& g : b->groups)
             if ((e = launch_stage(b, g, g.var, g.grid, k, s)) != cudaSuccess) return e;
-        for (const Group& g : b->groups)
-            if ((e = launch_pp(b, g, k, s)) != cudaSuccess) return e;
-    }
     for (const Group& g : b->groups)
     {
+        if (!g.nstab) continue;
         StabBatchArgs sb{g.d_stab, g.d_stab_clock, b->d_clock, g.d_stab_tiles, g.nstab};
         if ((e = launch_stab_batch(g.n, sb, s)) != cudaSuccess) return e;
     }
     for (const Group& g : b->groups)
-        if ((e = launch_pp(b, g, 3, s)) != cudaSuccess) return e;
+        if (g.unfused && (e = launch_pp(b, g, 3, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(b->d_active, 0, sizeof(int), s)) != cudaSuccess) return e;
     return launch_batch_clock(b->d_clock, b->count, b->d_active, s);
 }
@@ -352,6 +356,20 @@ int frsdg_batch_create(frsdg_handle* const* handles, int32_t count, double* cons
     for (int i = 0; i < count; ++i)
         clk[size_t(i)] = BatchClock{0.0, dt[i], t_end[i], 1, dt_scale ? 1 : 0, dt_scale ? dt_scale[i] : 0.0, 0ull, 0ll};
     if ((e = upload(&b->d_clock, clk)) != cudaSuccess) return fail_cuda(e, "batch clocks");
+    // stage-epilogue operands: the handle's filter, weights and floor, and the clock's
+    // wave-speed slot for adaptive steps
+    std::vector<PostArgs> post(static_cast<size_t>(count));
+    for (int i = 0; i < count; ++i)
+    {
+        const frsdg_handle* h = handles[i];
+        PostArgs& p = post[size_t(i)];
+        for (int q = 0; q < h->n * h->n; ++q) p.F[q] = h->st.F[q];
+        for (int q = 0; q < h->n; ++q) p.w[q] = h->re.w[q];
+        p.pp_eps = h->cfg.pp_eps;
+        p.detJ = nullptr;  // affine
+        p.amax = dt_scale ? &b->d_clock[i].amax : nullptr;
+    }
+    if ((e = upload(&b->d_post, post)) != cudaSuccess) return fail_cuda(e, "batch epilogue operands");
     if ((e = cudaMalloc(&b->d_active, sizeof(int))) != cudaSuccess) return fail_cuda(e, "batch counter");
     if ((e = cudaMallocHost(&b->h_active, sizeof(int))) != cudaSuccess) return fail_cuda(e, "batch counter");
     for (Group& g : b->groups)
@@ -372,6 +390,15 @@ int frsdg_batch_create(frsdg_handle* const* handles, int32_t count, double* cons
             in.a = h->a2;
             in.U = states[i];
             in.inst = i;
+            in.pa = b->d_post + i;
+            // stage epilogues: the limiter on every stage output; the last stage also
+            // runs an element-local post-step (filter) and yields the wave speed
+            const bool pp_on = h->cfg.pp_limit != 0;
+            const bool fused = h->cfg.apply_filter || !h->cfg.apply_weno;
+            in.post[0] = in.post[1] = pp_on ? POST_PP : 0;
+            in.fused_step = fused ? 1 : 0;
+            in.post[2] = (pp_on ? POST_PP : 0) |
+                         (fused ? (h->cfg.apply_filter ? POST_FILTER : 0) | (dt_scale ? POST_AMAX : 0) : 0);
             const size_t nt = size_t(h->ntot);
             for (int k = 0; k < 3; ++k)
             {
@@ -391,7 +418,9 @@ int frsdg_batch_create(frsdg_handle* const* handles, int32_t count, double* cons
             pa.row_base = 0;
             pa.U = in.U;
             pa.U32 = nullptr;
+            pa.fused = fused ? 1 : 0;
             pp.push_back(pa);
+            if (!fused) ++g.unfused;
             elem_begin.push_back(elem_begin.back() + h->nelem);
             for (int var = 0; var < 2; ++var)
             {
@@ -400,8 +429,10 @@ int frsdg_batch_create(frsdg_handle* const* handles, int32_t count, double* cons
                 for (int by = 0; by < (h->Ny + ty - 1) / ty; ++by)
                     for (int bx = 0; bx < (h->Nx + tx - 1) / tx; ++bx) tiles[var].push_back(make_int4(int(m), bx, by, 0));
             }
-            for (int by = 0; by < (h->Ny + sty - 1) / sty; ++by)
-                for (int bx = 0; bx < (h->Nx + stx - 1) / stx; ++bx) stiles.push_back(make_int4(int(m), bx, by, 0));
+            if (!fused)
+                for (int by = 0; by < (h->Ny + sty - 1) / sty; ++by)
+                    for (int bx = 0; bx < (h->Nx + stx - 1) / stx; ++bx)
+                        stiles.push_back(make_int4(int(m), bx, by, 0));
         }
         g.nelem = elem_begin.back();
         g.ntiles[0] = int(tiles[0].size());

@@ -152,6 +152,7 @@ static void free_handle(frsdg_handle* h)
     cudaFree(h->d_ynorm);
     cudaFree(h->d_bxy);
     cudaFree(h->d_detJ);
+    cudaFree(h->d_post);
     cudaFree(h->d_work);
     cudaFree(h->d_stage);
     cudaFree(h->d_bad);
@@ -515,6 +516,24 @@ int frsdg_create(const frsdg_config* cfg, frsdg_handle** out)
             }
         }
     }
+
+    // operands of the fused stage epilogue (frsdg_rk_stage_fused)
+    if (cfg->dim == 2)
+    {
+        PostArgs pa{};
+        for (int q = 0; q < n * n; ++q) pa.F[q] = h->st.F[q];
+        for (int q = 0; q < n; ++q) pa.w[q] = h->re.w[q];
+        pa.pp_eps = cfg->pp_eps;
+        pa.detJ = h->d_detJ;
+        pa.amax = nullptr;
+        cudaError_t e = cudaMalloc(&h->d_post, sizeof(PostArgs));
+        if (e == cudaSuccess) e = cudaMemcpy(h->d_post, &pa, sizeof(PostArgs), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess)
+        {
+            free_handle(h);
+            return cuda_fail(e, "stage epilogue operands");
+        }
+    }
     *out = h;
     return FRSDG_OK;
 }
@@ -672,6 +691,61 @@ int frsdg_rk_stage_mixed(frsdg_handle* h, double t, const double* Us, const doub
     if (!h || !Us || !out) return fail(FRSDG_ERR_ARG, "null argument");
     StageArgs st{A, B, acc, alpha, beta, gamma, delta, nullptr};
     return run_residual_f32(h, MODE_STAGE, t, Us, true, out, false, &st, stream);
+}
+
+static int run_pp_limit(frsdg_handle* h, double* U, float* U32, cudaStream_t s);
+
+int frsdg_rk_stage_fused(frsdg_handle* h, double t, const double* Us, const double* A, double alpha, const double* B,
+                         double beta, double gamma, double* out, double* acc, double delta, int32_t flags, void* stream)
+{
+    if (!h || !Us || !out) return fail(FRSDG_ERR_ARG, "null argument");
+    if (out == Us) return fail(FRSDG_ERR_ARG, "frsdg_rk_stage_fused: out must not alias Us");
+    if (flags & ~(FRSDG_STAGE_MIXED | FRSDG_STAGE_LIMIT | FRSDG_STAGE_POST_STEP))
+        return fail(FRSDG_ERR_ARG, "frsdg_rk_stage_fused: unknown flags");
+    if ((reinterpret_cast<uintptr_t>(Us) | reinterpret_cast<uintptr_t>(out) | reinterpret_cast<uintptr_t>(A) |
+         reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(acc)) & 15)
+        return fail(FRSDG_ERR_ARG, "device pointers must be 16-byte aligned");
+    const bool mixed = (flags & FRSDG_STAGE_MIXED) != 0;
+    const bool step = (flags & FRSDG_STAGE_POST_STEP) != 0;
+    const bool limit = (step || (flags & FRSDG_STAGE_LIMIT)) && h->cfg.pp_limit;
+    if (mixed && (h->cfg.dim != 2 || h->cfg.cond_sys))
+        return fail(FRSDG_ERR_UNSUPPORTED, "frsdg_rk_stage_fused: the mixed form needs a 2D configuration without "
+                                           "change of variables");
+    StageArgs st{A, B, acc, alpha, beta, gamma, delta, nullptr};
+    // the post-step is element-local unless it is the WENO limiter alone (the filter
+    // overrides WENO when both are set)
+    const bool local_step = h->cfg.apply_filter || !h->cfg.apply_weno;
+    if (h->cfg.dim == 2 && (!step || local_step))
+    {
+        int post = limit ? POST_PP : 0;
+        if (step && h->cfg.apply_filter) post |= POST_FILTER;
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        h->last = s;
+        Fr2dArgs a = h->a2;
+        a.t = t;
+        a.mode = MODE_STAGE;
+        a.cond_sys = 0;
+        a.U = Us;
+        a.W = nullptr;
+        a.out = out;
+        a.out_f32 = 0;
+        a.in_f64 = mixed ? 1 : 0;
+        a.st = st;
+        a.post = post;
+        a.pa = h->d_post;
+        apply_window(h, a);
+        const cudaError_t e = mixed ? dispatch2d<float>(h->n, h->cfg.gas_law, h->cfg.riemann, h->geo, a, s)
+                                    : dispatch2d<double>(h->n, h->cfg.gas_law, h->cfg.riemann, h->geo, a, s);
+        if (e != cudaSuccess) return cuda_fail(e, "fused stage launch");
+        return FRSDG_OK;
+    }
+    // 1D, or a post-step that reads neighbours: the stage, then the separate passes
+    int rc = mixed ? run_residual_f32(h, MODE_STAGE, t, Us, true, out, false, &st, stream)
+                   : run_residual(h, MODE_STAGE, t, Us, nullptr, out, stream, &st);
+    if (rc) return rc;
+    if (step) return frsdg_post_step(h, out, stream);
+    if (limit) return run_pp_limit(h, out, nullptr, static_cast<cudaStream_t>(stream));
+    return FRSDG_OK;
 }
 
 int frsdg_set_row_window(frsdg_handle* h, int row_base, int rows, int row_begin, int row_end)

@@ -76,6 +76,25 @@ struct GasParams
     double gamma, a, b;
 };
 
+// Stage epilogue of the 2D residual kernel (MODE_STAGE): element-local work fused into
+// the stage that produces a state, in this order -- the spectral filter of the
+// post-step (the whole-element form of stab2d_tile's filter branch), the positivity
+// limiter (pplimit.cuh), and the largest |v| + c of the result (adaptive time steps).
+enum : int
+{
+    POST_FILTER = 1,
+    POST_PP = 2,
+    POST_AMAX = 4
+};
+struct PostArgs
+{
+    double F[kMaxN * kMaxN];   // filter matrix, row-major (StabArgs::F)
+    double w[kMaxN];           // GLL weights
+    double pp_eps;             // the limiter's floor (cfg.pp_eps)
+    const double* detJ;        // per-node detJ [global element][node] (curved meshes), or null
+    unsigned long long* amax;  // POST_AMAX: atomicMax target (bits of a positive double)
+};
+
 struct Fr2dArgs
 {
     int    Nx, Ny, per_x, per_y;
@@ -105,6 +124,10 @@ struct Fr2dArgs
                        // 2 distance-2 colouring (i + 2 j) mod 5 for all five blocks of an element row
     int    in_f64;     // FP32 instantiation: U is an FP64 state, node primitives recovered in FP64
     Ops    ops;
+    // (after the operators: a batch launch sets these per stage, not per instance)
+    int    post;       // MODE_STAGE: element-local post-processing of the stage output (POST_*)
+    int    pad_post_;
+    const PostArgs* pa;  // its operands (device memory) when post != 0
 };
 
 // ---- batches of instances (batch.cu) ----------------------------------------
@@ -137,7 +160,10 @@ struct BatchInst2D
     double*  U;       // state
     double*  b[3];    // SSP-RK3 stage outputs (b[2]: the last, limited into U by the post-step)
     int      inst;    // batch index (clock)
+    int      fused_step;  // the post-step is the last stage's epilogue, which writes U
+    int      post[3];     // stage epilogue of each stage (Fr2dArgs::post)
     int      pad_;
+    const PostArgs* pa;   // its operands
 };
 
 struct Fr2dBatchArgs
@@ -217,6 +243,18 @@ template <class S, int N>
 cudaError_t launch_fr2d_batch(int gas, int riem, int var, const Fr2dBatchArgs& b, int grid, cudaStream_t s,
                               int* occupancy);
 
+// Stage combination alpha A + beta B + gamma rhs at index idx (rhs = -r), with the
+// accumulator update acc += delta rhs.
+__device__ __forceinline__ double stage_value(const StageArgs& st, int64_t idx, double r)
+{
+    const double v = -r;
+    double o = 0.0;
+    if (st.A) o = st.alpha * __ldg(st.A + idx);
+    if (st.B) o = o + st.beta * __ldg(st.B + idx);
+    if (st.acc) st.acc[idx] = st.acc[idx] + st.delta * v;
+    return o + st.gamma * v;
+}
+
 // Output of one real residual value r = R at index idx in the requested form.
 __device__ __forceinline__ void store_residual(int mode, const double* W, const StageArgs& st, double* out,
                                                int64_t idx, double r)
@@ -225,14 +263,9 @@ __device__ __forceinline__ void store_residual(int mode, const double* W, const 
     else if (mode == MODE_IFUNC) out[idx] = __ldg(W + idx) + r;
     else if (mode == MODE_STAGE)
     {
-        const double v = -r;
-        double o = 0.0;
-        if (st.A) o = st.alpha * __ldg(st.A + idx);
-        if (st.B) o = o + st.beta * __ldg(st.B + idx);
-        const double ov = o + st.gamma * v;
+        const double ov = stage_value(st, idx, r);
         out[idx] = ov;
         if (st.out32) st.out32[idx] = static_cast<float>(ov);
-        if (st.acc) st.acc[idx] = st.acc[idx] + st.delta * v;
     }
     else out[idx] = r;
 }

@@ -29,6 +29,7 @@ struct frsdg_handle
     double*      d_bxy = nullptr;
     double*      d_detJ = nullptr;   // positivity limiter on curved meshes: detJ per node
     frsdg::PPArgs       pp{};               // template of the positivity limiter's launch
+    frsdg::PostArgs*    d_post = nullptr;   // 2D: operands of the fused stage epilogue
     double*      d_work = nullptr;   // post-step source copy (WENO)
     double*      d_stage = nullptr;  // host-buffer staging (2 * ntot), allocated on first use
     unsigned long long* d_bad = nullptr;

@@ -1,20 +1,11 @@
-// pplimit.cu -- positivity-preserving scaling limiter (Zhang and Shu, "On
-// positivity-preserving high order discontinuous Galerkin schemes for compressible
-// Euler equations on rectangular meshes", J. Comput. Phys. 229 (2010) 8918-8934,
-// sec. 3), per element, in place:
-//   Ubar = GLL-quadrature cell average (weights w_k w_l detJ_kl in 2D, w_k in 1D),
-//   eps = min(eps0, rho_bar, p_bar); elements with an inadmissible average are kept;
-//   1. rho_min < eps:  rho <- rho_bar + theta1 (rho - rho_bar),
-//                      theta1 = (rho_bar - eps) / (rho_bar - rho_min);
-//   2. U <- Ubar + theta2 (U - Ubar), theta2 = min over nodes with p < eps of the
-//      point t of the segment Ubar -> U_q with pressure eps (60 bisection steps,
-//      keeping the admissible end).
-// It has no counterpart in the reference.  Elements that need no limiting are not
-// written back, so the pass reads the state once and writes only limited elements.
+// pplimit.cu -- the positivity-preserving scaling limiter's kernels (the per-element
+// limiter itself is in pplimit.cuh).  Elements that need no limiting are not written
+// back, so a pass reads the state once and writes only limited elements.
 //
 // 2D: one warp per element (lanes over its nodes, shuffles for the cell sums and
 // the minima); 1D: one thread per element.
 #include "pplimit.hpp"
+#include "pplimit.cuh"
 #include "device_math.cuh"
 
 #include <cuda_runtime.h>
@@ -23,160 +14,6 @@ namespace frsdg
 {
 namespace
 {
-
-__device__ __forceinline__ double pp_gas_pressure(const PPArgs& a, double rho, double e)
-{
-    if (a.gas_law == FRSDG_GAS_IDEAL) return (a.gas.gamma - 1.0) * rho * e;
-    const double covol = 1.0 - a.gas.b * rho;
-    const double cvT = e + a.gas.a * rho;
-    return ((a.gas.gamma - 1.0) * rho * cvT) / covol - a.gas.a * rho * rho;
-}
-
-template <int NV> __device__ __forceinline__ double pp_pressure(const PPArgs& a, const double* u)
-{
-    double m2 = 0.0;
-#pragma unroll
-    for (int c = 1; c < NV - 1; ++c) m2 += u[c] * u[c];
-    const double rho = u[0];
-    const double e = (u[NV - 1] - 0.5 * m2 / rho) / rho;
-    return pp_gas_pressure(a, rho, e);
-}
-
-// |v| + c of a node (the sound speed of the configured gas law, c^2 clamped at 0)
-__device__ __forceinline__ double node_wave_speed(const PPArgs& a, const double* u)
-{
-    const double rho = u[0];
-    const double vx = u[1] / rho, vy = u[2] / rho;
-    const double e = u[3] / rho - 0.5 * (vx * vx + vy * vy);
-    double c2;
-    if (a.gas_law == FRSDG_GAS_IDEAL) c2 = a.gas.gamma * (a.gas.gamma - 1.0) * e;
-    else
-    {
-        const double cov = 1.0 - a.gas.b * rho, gm1 = a.gas.gamma - 1.0;
-        c2 = (a.gas.gamma * gm1 * (e + a.gas.a * rho)) / (cov * cov) +
-             (gm1 * a.gas.a * rho * (2.0 - a.gas.b * rho)) / (cov * cov) - 2.0 * a.gas.a * rho;
-    }
-    return sqrt(vx * vx + vy * vy) + sqrt(fmax(c2, 0.0));
-}
-
-template <int NV>
-__device__ __forceinline__ double pp_segment_root(const PPArgs& a, const double* ub, const double* uq, double eps)
-{
-    double lo = 0.0, hi = 1.0, s[NV];
-    for (int it = 0; it < 60; ++it)
-    {
-        const double mid = 0.5 * (lo + hi);
-#pragma unroll
-        for (int c = 0; c < NV; ++c) s[c] = ub[c] + mid * (uq[c] - ub[c]);
-        if (s[0] > 0.0 && pp_pressure<NV>(a, s) >= eps) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
-__device__ __forceinline__ double warp_sum(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-__device__ __forceinline__ double warp_min(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-
-// One element of a 2D state, limited by one warp: base / base32 point at the element's
-// values (base32 may be null), e_glob is its global index for the cached detJ;
-// refresh32: write the FP32 copy even when the element is admissible.
-template <int N>
-__device__ __forceinline__ void pp_element2d(const PPArgs& a, double* base, float* base32, int64_t e_glob,
-                                             bool limit, bool refresh32, unsigned long long* amax = nullptr)
-{
-    constexpr int NQ = N * N, R = (NQ + 31) / 32;
-    const int lane = threadIdx.x & 31;
-    double u[R][4], W[R];
-    double wsum = 0.0, ub[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int r = 0; r < R; ++r)
-    {
-        const int q = lane + 32 * r;
-        W[r] = 0.0;
-        u[r][0] = u[r][1] = u[r][2] = u[r][3] = 0.0;
-        if (q < NQ)
-        {
-            const double2 x0 = *reinterpret_cast<const double2*>(base + q * 4);
-            const double2 x1 = *reinterpret_cast<const double2*>(base + q * 4 + 2);
-            u[r][0] = x0.x; u[r][1] = x0.y; u[r][2] = x1.x; u[r][3] = x1.y;
-            W[r] = a.w[q % N] * a.w[q / N] * (a.detJ ? __ldg(a.detJ + e_glob * NQ + q) : 1.0);
-        }
-        wsum += W[r];
-#pragma unroll
-        for (int c = 0; c < 4; ++c) ub[c] += W[r] * u[r][c];
-    }
-    wsum = warp_sum(wsum);
-#pragma unroll
-    for (int c = 0; c < 4; ++c) ub[c] = warp_sum(ub[c]) / wsum;
-    const double pb = pp_pressure<4>(a, ub);
-    bool touched = false;
-    // the limiter acts when enabled and the cell average is admissible (uniform across the warp)
-    if (limit && ub[0] > 0.0 && pb > 0.0)
-    {
-        const double eps = fmin(a.eps0, fmin(ub[0], pb));
-        double rmin = 1e300;
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-            if (lane + 32 * r < NQ) rmin = fmin(rmin, u[r][0]);
-        rmin = warp_min(rmin);
-        if (rmin < eps)
-        {
-            const double th1 = (ub[0] - eps) / (ub[0] - rmin);
-#pragma unroll
-            for (int r = 0; r < R; ++r) u[r][0] = ub[0] + th1 * (u[r][0] - ub[0]);
-            touched = true;
-        }
-        double th2 = 1.0;
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-            if (lane + 32 * r < NQ && !(pp_pressure<4>(a, u[r]) >= eps)) th2 = fmin(th2, pp_segment_root<4>(a, ub, u[r], eps));
-        th2 = warp_min(th2);
-        if (th2 < 1.0)
-        {
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-                for (int c = 0; c < 4; ++c) u[r][c] = ub[c] + th2 * (u[r][c] - ub[c]);
-            touched = true;
-        }
-    }
-    if (amax)
-    {
-        // the largest |v| + c of the (limited) element, for the next adaptive time step
-        double w = 0.0;
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-            if (lane + 32 * r < NQ) w = fmax(w, node_wave_speed(a, u[r]));
-        w = -warp_min(-w);
-        if (lane == 0 && w > 0.0 && w < 1e300) atomicMax(amax, static_cast<unsigned long long>(__double_as_longlong(w)));
-    }
-    if (!touched && !refresh32) return;
-#pragma unroll
-    for (int r = 0; r < R; ++r)
-    {
-        const int q = lane + 32 * r;
-        if (q >= NQ) continue;
-        if (touched)
-        {
-            *reinterpret_cast<double2*>(base + q * 4) = make_double2(u[r][0], u[r][1]);
-            *reinterpret_cast<double2*>(base + q * 4 + 2) = make_double2(u[r][2], u[r][3]);
-        }
-        if (base32)
-            *reinterpret_cast<float4*>(base32 + q * 4) =
-                make_float4(float(u[r][0]), float(u[r][1]), float(u[r][2]), float(u[r][3]));
-    }
-}
-
 template <int N> __global__ void __launch_bounds__(256) pp_limit2d_kernel(const PPArgs a)
 {
     constexpr int NQ = N * N;
@@ -204,6 +41,7 @@ template <int N> __global__ void __launch_bounds__(256) pp_batch_kernel(const PP
     const BatchInst2D& in = b.binst[lo];
     if (!b.clock[in.inst].active) return;
     const PPArgs& a = b.inst[lo];
+    if (a.fused) return;
     const int64_t e = g - b.elem_begin[lo];
     // slots 0-2: the stage outputs; 3: the state after the post-step
     double* buf = b.slot == 3 ? in.U : in.b[b.slot];

@@ -18,7 +18,7 @@ struct PPArgs
     double*   U;            // state, limited in place
     float*    U32;          // optional FP32 copy of U, refreshed where U changes (2D)
     int       enabled;      // cfg.pp_limit
-    int       pad_;
+    int       fused;        // batch: the instance's stage epilogues limit it (the limiter passes skip it)
 };
 
 // Positivity limiter over a batch group (affine 2D instances of one order): warp per
@@ -33,6 +33,7 @@ struct PPBatchArgs
     BatchClock*        clock;       // per batch instance; the limiter pass of the state gathers its
                                     // max |v| + c into clock[i].amax (adaptive time steps)
     int                slot;        // 0-2: stage output b[slot]; 3: the state U after the post-step
+                                    // (instances whose PPArgs::fused is set are skipped)
     int                pad_;
 };
 cudaError_t launch_pp_batch(int n, const PPBatchArgs& b, cudaStream_t s);

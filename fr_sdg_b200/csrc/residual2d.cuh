@@ -22,6 +22,7 @@
 #include "device_math.cuh"
 #include "frsdg_internal.hpp"
 #include "physics.cuh"
+#include "pplimit.cuh"
 
 namespace frsdg
 {
@@ -99,6 +100,13 @@ template <class S, int N, int GEO, int VAR = 0> struct Tile2D
     static constexpr int nS   = oDel + TE * 16 * N;
     static constexpr size_t seed_bytes = JVP ? sizeof(double) * 4 * TE * NN : 0;
     static constexpr size_t bytes = size_t(nS) * sizeof(S) + seed_bytes;
+    // stage epilogue (Fr2dArgs::post): the tile's stage outputs, [element][node][eq]
+    // doubles, go to the face-record region (dead after P2) when it is large enough,
+    // else after the rest; the filter writes its result over the flux region (dead
+    // after P3)
+    static constexpr size_t post_bytes = size_t(TE) * 4 * NN * sizeof(double);
+    static constexpr bool POST_IN_REC = size_t(RF_N) * NREC * sizeof(S) >= post_bytes;
+    static constexpr size_t bytes_post = POST_IN_REC ? bytes : bytes + post_bytes;
     // index of boundary node (k, l) among an element's NB boundary nodes:
     // bottom row, top row, then the interior of the left and right columns
     __host__ __device__ static constexpr int bidx(int k, int l)
@@ -405,10 +413,77 @@ __device__ __forceinline__ void face_jumps(const Fr2dArgs& a, int i0, int j0, bo
     }
 }
 
+// Stage epilogue of a tile (Fr2dArgs::post, MODE_STAGE): sO holds the stage outputs of
+// the tile's elements; the spectral filter of the post-step (stab2d_tile's filter
+// branch, SpectralFilter::apply_filter, filter.hpp:425-445: half the sum of the filter
+// along the element's rows and along its columns), the positivity limiter and the
+// wave-speed maximum act on each element in shared memory, then the tile is stored.
+template <class T, int N, int GAS>
+__device__ __forceinline__ void stage_epilogue(const Fr2dArgs& a, int i0, int j0, int txe, int tye, double* sO,
+                                               unsigned char* smem_raw)
+{
+    constexpr int TX = T::TX, TE = T::TE, BT = T::BT, NN = N * N, ND = 4 * NN;
+    static_assert(BT % 32 == 0, "whole warps");
+    const int tid = threadIdx.x;
+    const PostArgs& P = *a.pa;
+    double* sX = sO;
+    if (a.post & POST_FILTER)
+    {
+        double* sY = reinterpret_cast<double*>(smem_raw);
+#pragma unroll 1
+        for (int dir = 0; dir < 2; ++dir)
+        {
+            for (int t = tid; t < TE * 4 * N; t += BT)
+            {
+                const int eq = t % 4, m = (t / 4) % N, e = t / (4 * N);
+                if (e % TX >= txe || e / TX >= tye) continue;
+                const double* src = sO + e * ND + eq;
+                double cv[N];
+#pragma unroll
+                for (int c = 0; c < N; ++c) cv[c] = src[(dir == 0 ? m * N + c : c * N + m) * 4];
+#pragma unroll
+                for (int r = 0; r < N; ++r)
+                {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int c = 0; c < N; ++c) acc += __ldg(&P.F[r * N + c]) * cv[c];
+                    double& d = sY[e * ND + (dir == 0 ? m * N + r : r * N + m) * 4 + eq];
+                    d = dir == 0 ? acc : 0.5 * (d + acc);
+                }
+            }
+            __syncthreads();
+        }
+        sX = sY;
+    }
+    if (a.post & (POST_PP | POST_AMAX))
+    {
+        const PPView v{GAS == 0 ? FRSDG_GAS_IDEAL : FRSDG_GAS_VDW, a.gas, P.pp_eps, P.w, P.detJ};
+        unsigned long long* amax = (a.post & POST_AMAX) ? P.amax : nullptr;
+        for (int e = tid / 32; e < TE; e += BT / 32)
+        {
+            const int tx = e % TX, ty = e / TX;
+            if (tx >= txe || ty >= tye) continue;  // uniform across the warp
+            const int64_t e_glob = int64_t(j0 + ty + a.row_base) * a.Nx + (i0 + tx);
+            pp_element2d<N>(v, sX + e * ND, nullptr, e_glob, (a.post & POST_PP) != 0, false, amax);
+        }
+        __syncthreads();
+    }
+    double* out = static_cast<double*>(a.out);
+    for (int q = tid; q < TE * (ND / 2); q += BT)
+    {
+        const int e = q / (ND / 2), k = q % (ND / 2), tx = e % TX, ty = e / TX;
+        if (tx >= txe || ty >= tye) continue;
+        reinterpret_cast<double2*>(out + (int64_t(j0 + ty) * a.Nx + (i0 + tx)) * ND)[k] =
+            reinterpret_cast<const double2*>(sX + e * ND)[k];
+    }
+}
+
 // One tile of the residual pass: tile (bx, by) of element columns/rows (the Jacobian
 // slice of MODE_JAC is blockIdx.z), with the launch arguments `a` and the operators
 // `ops`; smem_raw is the CTA's dynamic shared memory (T::bytes).
-template <class S, int N, int GAS, int RIEM, int GEO, int VAR>
+// POST: the instantiation with the stage epilogue (Fr2dArgs::post); the others carry no
+// epilogue code, which would otherwise cost the main path registers.
+template <class S, int N, int GAS, int RIEM, int GEO, int VAR, bool POST = false>
 __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int bx, int by, unsigned char* smem_raw)
 {
     using T = Tile2D<S, N, GEO, VAR>;
@@ -421,6 +496,9 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
     S* sC   = sm + T::oC;
     S* sRec = sm + T::oRec;
     S* sDel = sm + T::oDel;
+    // stage epilogue: the tile's stage outputs (Tile2D::POST_IN_REC)
+    const bool post = POST && !T::JVP && a.mode == MODE_STAGE && a.post != 0;
+    double* sO = reinterpret_cast<double*>(smem_raw + (T::POST_IN_REC ? T::oRec * sizeof(S) : T::bytes));
     double* sSeed = reinterpret_cast<double*>(smem_raw + size_t(T::nS) * sizeof(S));
 
     const int tid = threadIdx.x;
@@ -743,27 +821,38 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
             }
             else if (a.out_f32)
                 reinterpret_cast<float*>(a.out)[gidx] = static_cast<float>(s_re(R));
+            else if (post)
+                sO[e * ND + (l * N + k) * 4 + eq] = stage_value(a.st, gidx, s_re(R));
             else
             {
                 store_residual(a.mode, a.W, a.st, out, gidx, s_re(R));
             }
         }
     }
+    if constexpr (POST && !T::JVP)
+    {
+        if (post)
+        {
+            __syncthreads();
+            stage_epilogue<T, N, GAS>(a, i0, j0, txe, tye, sO, smem_raw);
+        }
+    }
 }
 
-template <class S, int N, int GAS, int RIEM, int GEO>
+template <class S, int N, int GAS, int RIEM, int GEO, bool POST>
 __global__ void __launch_bounds__((Tile2D<S, N, GEO>::BT)) __maxnreg__((Tile2D<S, N, GEO>::MAXREG))
 fr2d_kernel(const __grid_constant__ Fr2dArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    fr2d_tile<S, N, GAS, RIEM, GEO, 0>(a, a.ops, blockIdx.x, blockIdx.y, smem_raw);
+    fr2d_tile<S, N, GAS, RIEM, GEO, 0, POST>(a, a.ops, blockIdx.x, blockIdx.y, smem_raw);
 }
 
-template <class S, int N, int GAS, int RIEM, int GEO>
-cudaError_t launch_fr2d_kernel(const Fr2dArgs& a, cudaStream_t st)
+template <class S, int N, int GAS, int RIEM, int GEO, bool POST>
+cudaError_t launch_fr2d_kernel_v(const Fr2dArgs& a, cudaStream_t st)
 {
     using T = Tile2D<S, N, GEO>;
-    auto kern = fr2d_kernel<S, N, GAS, RIEM, GEO>;
+    auto kern = fr2d_kernel<S, N, GAS, RIEM, GEO, POST>;
+    constexpr size_t bytes = POST ? T::bytes_post : T::bytes;
     // kernel attributes are per device: set them once on each device that launches
     static bool attr_done[64] = {};
     int dev = 0;
@@ -771,7 +860,7 @@ cudaError_t launch_fr2d_kernel(const Fr2dArgs& a, cudaStream_t st)
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64 || !attr_done[dev])
     {
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(T::bytes));
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
         if (e != cudaSuccess) return e;
         e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
@@ -779,8 +868,18 @@ cudaError_t launch_fr2d_kernel(const Fr2dArgs& a, cudaStream_t st)
     }
     dim3 grid((a.Nx + T::TX - 1) / T::TX, (a.row_end - a.row_begin + T::TY - 1) / T::TY,
               a.mode == MODE_JAC ? (a.jac_cmode == 2 ? 5 : a.jac_cmode ? 9 : 2) * T::NN * 4 : 1);
-    kern<<<grid, T::BT, T::bytes, st>>>(a);
+    kern<<<grid, T::BT, bytes, st>>>(a);
     return cudaGetLastError();
+}
+
+template <class S, int N, int GAS, int RIEM, int GEO>
+cudaError_t launch_fr2d_kernel(const Fr2dArgs& a, cudaStream_t st)
+{
+    if constexpr (scalar_traits<S>::words == 1)
+    {
+        if (a.mode == MODE_STAGE && a.post) return launch_fr2d_kernel_v<S, N, GAS, RIEM, GEO, true>(a, st);
+    }
+    return launch_fr2d_kernel_v<S, N, GAS, RIEM, GEO, false>(a, st);
 }
 
 // ---- batches ------------------------------------------------------------------
@@ -789,7 +888,9 @@ cudaError_t launch_fr2d_kernel(const Fr2dArgs& a, cudaStream_t st)
 //   k = 0: b0 = U + h L(U);  k = 1: b1 = 3/4 U + 1/4 b0 + h/4 L(b0);
 //   k = 2: b2 = 1/3 U + 2/3 b1 + 2h/3 L(b1).
 // The mixed form (FP32 instantiation) reads the same FP64 stage inputs and recovers
-// every node's primitives in FP64 (Fr2dArgs::in_f64).
+// every node's primitives in FP64 (Fr2dArgs::in_f64).  Each stage output passes the
+// instance's stage epilogue (post[k]); with fused_step the last one is the whole
+// post-step and the stage writes the state itself.
 __device__ __forceinline__ void batch_stage_args(Fr2dArgs& a, const BatchInst2D& in, const BatchClock& ck, int k,
                                                  bool mixed)
 {
@@ -803,6 +904,8 @@ __device__ __forceinline__ void batch_stage_args(Fr2dArgs& a, const BatchInst2D&
     a.st.delta = 0.0;
     a.st.out32 = nullptr;
     a.st.A = in.U;
+    a.post = in.post[k];
+    a.pa = in.pa;
     if (k == 0)
     {
         a.U = in.U;
@@ -826,7 +929,7 @@ __device__ __forceinline__ void batch_stage_args(Fr2dArgs& a, const BatchInst2D&
     else
     {
         a.U = in.b[1];
-        a.out = in.b[2];
+        a.out = in.fused_step ? in.U : in.b[2];
         a.st.B = in.b[1];
         a.st.alpha = 1.0 / 3.0;
         a.st.beta = 2.0 / 3.0;
@@ -859,7 +962,7 @@ fr2d_batch_kernel(const __grid_constant__ Fr2dBatchArgs b)
         __syncthreads();
         if (threadIdx.x == 0) batch_stage_args(sa, in, ck, b.stage, b.mixed != 0);
         __syncthreads();
-        fr2d_tile<S, N, GAS, RIEM, GEO_AFFINE, VAR>(sa, b.ops, tm.y, tm.z, smem_raw);
+        fr2d_tile<S, N, GAS, RIEM, GEO_AFFINE, VAR, true>(sa, b.ops, tm.y, tm.z, smem_raw);
     }
 }
 
@@ -874,14 +977,14 @@ cudaError_t launch_fr2d_batch_kernel(const Fr2dBatchArgs& b, int grid, cudaStrea
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64 || !attr_done[dev])
     {
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(T::bytes));
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(T::bytes_post));
         if (e != cudaSuccess) return e;
         e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) attr_done[dev] = true;
     }
-    if (occupancy) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, kern, T::BT, T::bytes);
-    if (grid > 0 && b.ntiles > 0) kern<<<grid, T::BT, T::bytes, st>>>(b);
+    if (occupancy) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, kern, T::BT, T::bytes_post);
+    if (grid > 0 && b.ntiles > 0) kern<<<grid, T::BT, T::bytes_post, st>>>(b);
     return cudaGetLastError();
 }
 

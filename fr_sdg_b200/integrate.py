@@ -99,41 +99,51 @@ class Integrator:
         # the positivity limiter (cfg.pp_limit) acts on every stage output; the
         # post-step applies it again after the stabilisation
         self.pp = bool(cfg.pp_limit)
+        # an element-local post-step (the filter overrides WENO when both are set) is
+        # fused into the last stage of every step
+        self.local_post = bool(cfg.apply_filter or not cfg.apply_weno) and (self.stabilise or self.pp)
 
     def _buffers(self, U: torch.Tensor):
         if self._buf is None or self._buf[0].device != U.device:
             self._buf = [torch.empty_like(U) for _ in range(3)]
         return self._buf
 
-    def _rk(self, t: float, Us: torch.Tensor, out: torch.Tensor, **kw) -> None:
+    def _rk(self, t: float, Us: torch.Tensor, out: torch.Tensor, post_step: bool = False, **kw) -> None:
+        """One stage; the positivity limiter on its output and, with post_step, the whole
+        post-step run in the stage's launch (frsdg_rk_stage_fused)."""
         if self.before is not None:
             self.before(Us)
-        if self.mixed:
-            self.s.rk_stage_mixed(t, Us, out, **kw)
+        flags = (A.STAGE_MIXED if self.mixed else 0) | (A.STAGE_LIMIT if self.pp else 0)
+        if post_step:
+            flags |= A.STAGE_POST_STEP
+        if flags:
+            self.s.rk_stage_fused(t, Us, out, flags, **kw)
         else:
             self.s.rk_stage(t, Us, out, **kw)
-        if self.pp:
-            self.s.pp_limit(out)
 
     def step(self, U: torch.Tensor, t: float, dt: float) -> None:
-        """Advance U (in place) from t to t + dt, then apply the post-step limiter."""
+        """Advance U (in place) from t to t + dt, then apply the post-step limiter.  An
+        element-local post-step (the filter, the positivity limiter) runs inside the last
+        stage's launch, which then writes U itself; the WENO limiter, which reads the
+        neighbours, runs after it as its own pass."""
         s = self.s
         b1, b2, b3 = self._buffers(U)[:3]
-        # with a limiter, the last stage goes to a free buffer and the limiter writes U
-        # from it (frsdg_post_step_to: no device copy of the state)
+        fuse = self.local_post  # the last stage writes U through the post-step
+        separate = self.stabilise and not fuse
         if self.scheme == "ssprk3":
-            last = b3 if self.stabilise else U
+            last = b3 if separate else U
             self._rk(t, U, b1, gamma=dt, a=U, alpha=1.0)
             self._rk(t + dt, b1, b2, gamma=0.25 * dt, a=U, alpha=0.75, b=b1, beta=0.25)
-            self._rk(t + 0.5 * dt, b2, last, gamma=2.0 * dt / 3.0, a=U, alpha=1.0 / 3.0, b=b2, beta=2.0 / 3.0)
+            self._rk(t + 0.5 * dt, b2, last, post_step=fuse, gamma=2.0 * dt / 3.0, a=U, alpha=1.0 / 3.0, b=b2,
+                     beta=2.0 / 3.0)
         else:
-            last = b2 if self.stabilise else U
+            last = b2 if separate else U
             b3.copy_(U)
             self._rk(t, U, b1, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 6.0)
             self._rk(t + 0.5 * dt, b1, b2, gamma=0.5 * dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
             self._rk(t + 0.5 * dt, b2, b1, gamma=dt, a=U, alpha=1.0, acc=b3, delta=dt / 3.0)
-            self._rk(t + dt, b1, last, gamma=dt / 6.0, a=b3, alpha=1.0)
-        if self.stabilise:
+            self._rk(t + dt, b1, last, post_step=fuse, gamma=dt / 6.0, a=b3, alpha=1.0)
+        if separate:
             if self.before is not None:
                 self.before(last)
             s.apply_stabilization_to(last, U)

@@ -94,6 +94,16 @@ class FRSolver:
         A.check(self._lib.frsdg_rk_stage(self._h, t, _ptr(Us), p(a), alpha, p(b), beta, gamma, _ptr(out),
                                          p(acc), delta, _stream()), "frsdg_rk_stage")
 
+    def rk_stage_fused(self, t: float, Us: torch.Tensor, out: torch.Tensor, flags: int, gamma: float,
+                       a: torch.Tensor | None = None, alpha: float = 0.0, b: torch.Tensor | None = None,
+                       beta: float = 0.0, acc: torch.Tensor | None = None, delta: float = 0.0) -> None:
+        """rk_stage with the element-local work after it in the same launch (flags: A.STAGE_*):
+        the mixed residual, the positivity limiter on out, or the whole post-step on out."""
+        self._check_vec(Us, out, *(v for v in (a, b, acc) if v is not None))
+        p = lambda v: _ptr(v) if v is not None else None
+        A.check(self._lib.frsdg_rk_stage_fused(self._h, t, _ptr(Us), p(a), alpha, p(b), beta, gamma, _ptr(out),
+                                               p(acc), delta, int(flags), _stream()), "frsdg_rk_stage_fused")
+
     def _check_f32(self, *vs: torch.Tensor) -> None:
         for v in vs:
             if v.dtype != torch.float32 or not v.is_cuda or not v.is_contiguous() or v.numel() != self.n_dofs:

@@ -206,6 +206,26 @@ int frsdg_rk_stage_mixed(frsdg_handle* h, double t, const double* Us, const doub
                          const double* B, double beta, double gamma, double* out, double* acc,
                          double delta, void* stream);
 
+/* One Runge-Kutta stage with the element-local work that follows it fused in (no
+ * reference counterpart: the reference runs the post-step as a separate pass after
+ * TSStep, petsc_solver_impl.hpp:683-702).  out = alpha*A + beta*B + gamma*rhs(Us) and
+ * acc += delta*rhs as in frsdg_rk_stage, then per flag:
+ *   FRSDG_STAGE_MIXED      the residual of frsdg_rk_stage_mixed (2D, no change of variables);
+ *   FRSDG_STAGE_LIMIT      out = the positivity limiter applied to out (cfg.pp_limit);
+ *   FRSDG_STAGE_POST_STEP  out = frsdg_post_step applied to out (the spectral filter of
+ *                          cfg.apply_filter, then the limiter of cfg.pp_limit) -- the last
+ *                          stage of a step.
+ * In 2D, when the post-step is element-local (the filter, the limiter, or nothing; not
+ * the WENO limiter alone, which reads neighbours), this is ONE launch: each CTA
+ * finishes its elements' stage values in shared memory, filters and limits them there
+ * and writes out once.  Otherwise (1D, WENO) it runs the stage and then the separate
+ * passes.  Results equal the unfused sequence's up to rounding.  out may alias A (the
+ * state updated in place) but not Us. */
+enum { FRSDG_STAGE_MIXED = 1, FRSDG_STAGE_LIMIT = 2, FRSDG_STAGE_POST_STEP = 4 };
+int frsdg_rk_stage_fused(frsdg_handle* h, double t, const double* Us, const double* A, double alpha,
+                         const double* B, double beta, double gamma, double* out, double* acc,
+                         double delta, int32_t flags, void* stream);
+
 /* Element-diagonal blocks of the implicit Jacobian J = sigma*dM/dU + dR(M(U))/dU at
  * (t, U), by complex step (h = cfg.csd_eps) with element colouring, in one launch:
  * the preconditioner's part of ComplexStepJacobianStrategy::pre_jv_eval

@@ -9,6 +9,7 @@ from types import SimpleNamespace
 import pytest
 import torch
 
+from fr_sdg_b200 import _abi as A
 from fr_sdg_b200.integrate import Integrator
 
 
@@ -36,6 +37,15 @@ class DecaySolver:
         self.stages += 1
         if gamma > self.unstable_above:
             self._bad += 1
+
+    def rk_stage_fused(self, t, Us, out, flags, **kw):
+        """frsdg_rk_stage_fused: the stage, then the post-step (filter) and the limiter."""
+        self.rk_stage(t, Us, out, **kw)
+        step = bool(flags & A.STAGE_POST_STEP)
+        if step and (self.cfg.apply_filter or self.cfg.apply_weno):
+            self.limits += 1
+        if self.cfg.pp_limit and (step or flags & A.STAGE_LIMIT):
+            self.pp_calls.append(out.data_ptr())
 
     def apply_stabilization(self, U):
         self.limits += 1
@@ -138,11 +148,21 @@ def test_clipped_final_step_and_monitor_schedule():
 
 
 def test_before_stage_hook_sees_every_stage_input_and_the_limiter_input():
+    """The ghost-row hook runs before every stage and, when the post-step reads the
+    neighbours (WENO alone), before it; an element-local post-step (the filter) is part
+    of the last stage's launch and needs no refresh."""
     s = DecaySolver(limiter=True)
+    s.cfg.apply_filter, s.cfg.apply_weno = 0, 1
     U = torch.ones(4, dtype=torch.float64)
     calls = []
     Integrator(s, "ssprk3", before_stage=lambda V: calls.append(V.data_ptr())).step(U, 0.0, 0.1)
     assert len(calls) == 4 and calls[0] == U.data_ptr() and calls[3] != U.data_ptr()
+    assert s.limits == 1
+    s = DecaySolver(limiter=True)
+    calls = []
+    Integrator(s, "ssprk3", before_stage=lambda V: calls.append(V.data_ptr())).step(U, 0.0, 0.1)
+    assert len(calls) == 3 and calls[0] == U.data_ptr()
+    assert s.limits == 1
 
 
 def test_cfl_time_step_uniform_states():
