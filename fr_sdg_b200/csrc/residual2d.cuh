@@ -481,6 +481,21 @@ __device__ __forceinline__ void stage_epilogue(const Fr2dArgs& a, int i0, int j0
 // One tile of the residual pass: tile (bx, by) of element columns/rows (the Jacobian
 // slice of MODE_JAC is blockIdx.z), with the launch arguments `a` and the operators
 // `ops`; smem_raw is the CTA's dynamic shared memory (T::bytes).
+// FP32 derivatives: the rows of the rounded differentiation matrix do not sum to zero
+// exactly, so a line's constant part (a uniform background flux) would leave a residual
+// of ~1e-7 |F| |D| at every node, the same sign every step.  Differentiating the line
+// minus its first value removes that bias (D 1 = 0 in exact arithmetic, so the result
+// is unchanged otherwise).  FP64 keeps the reference's form.
+template <class S, int N> __device__ __forceinline__ void center_line(S (&v)[N])
+{
+    if constexpr (sizeof(S) == 4)
+    {
+        const S b = v[0];
+#pragma unroll
+        for (int m = 0; m < N; ++m) v[m] = v[m] - b;
+    }
+}
+
 // POST: the instantiation with the stage epilogue (Fr2dArgs::post); the others carry no
 // epilogue code, which would otherwise cost the main path registers.
 template <class S, int N, int GAS, int RIEM, int GEO, int VAR, bool POST = false>
@@ -666,12 +681,14 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
         S gv[N];
 #pragma unroll
         for (int m = 0; m < N; ++m) gv[m] = Gc[m * N];
+        center_line<S, N>(gv);
         if constexpr (GEO == GEO_CURVED)
         {
             const S* Fc = sF + (e * 4 + eq) * NN + k;
             S fv[N];
 #pragma unroll
             for (int m = 0; m < N; ++m) fv[m] = Fc[m * N];
+            center_line<S, N>(fv);
             const double* mt = a.metrics + ((int64_t(j0 + e / TX + a.row_base) * Nx + (i0 + e % TX)) * NN + k) * 4 + 2;
 #pragma unroll
             for (int l = 0; l < N; ++l)
@@ -762,6 +779,7 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
         S fv[N];
 #pragma unroll
         for (int m = 0; m < N; ++m) fv[m] = Fr[m];
+        center_line<S, N>(fv);
         const R_t dLl = opL<R_t>(ops, l), dRl = opR<R_t>(ops, l);
         const S dxl = sDel[((e * 4 + 0) * 4 + eq) * N + l];
         const S dxr = sDel[((e * 4 + 1) * 4 + eq) * N + l];
@@ -783,6 +801,7 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
             const S* Gr = sG + (e * 4 + eq) * NN + l * N;
 #pragma unroll
             for (int m = 0; m < N; ++m) gr[m] = Gr[m];
+            center_line<S, N>(gr);
         }
 #pragma unroll
         for (int k = 0; k < N; ++k)
