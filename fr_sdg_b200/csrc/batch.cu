@@ -354,7 +354,8 @@ int frsdg_batch_create(frsdg_handle* const* handles, int32_t count, double* cons
     // clocks
     std::vector<BatchClock> clk(static_cast<size_t>(count));
     for (int i = 0; i < count; ++i)
-        clk[size_t(i)] = BatchClock{0.0, dt[i], t_end[i], 1, dt_scale ? 1 : 0, dt_scale ? dt_scale[i] : 0.0, 0ull, 0ll};
+        clk[size_t(i)] = BatchClock{0.0, dt[i], t_end[i], 1, dt_scale ? 1 : 0, dt_scale ? dt_scale[i] : 0.0, 0ull, 0ll,
+                                    1e-3 * dt[i]};
     if ((e = upload(&b->d_clock, clk)) != cudaSuccess) return fail_cuda(e, "batch clocks");
     // stage-epilogue operands: the handle's filter, weights and floor, and the clock's
     // wave-speed slot for adaptive steps

@@ -144,6 +144,9 @@ struct BatchClock
     double dt_scale;
     unsigned long long amax;
     long long steps;   // steps taken
+    // adaptive: an instance whose step falls below dt_floor (a blown-up state's wave
+    // speed) stops where it is -- inactive before t_end -- instead of crawling on
+    double dt_floor;
 };
 
 __host__ __device__ inline double batch_step_size(const BatchClock& c)

@@ -70,6 +70,7 @@ __global__ void batch_clock_kernel(BatchClock* clock, int count, int* active_cou
                 const double w = __longlong_as_double(static_cast<long long>(c.amax));
                 if (c.amax && w > 0.0) c.dt = c.dt_scale / w;
                 c.amax = 0ull;
+                if (!(c.dt >= c.dt_floor)) c.active = 0;  // stalled (also a NaN step)
             }
             clock[i] = c;
         }

@@ -341,7 +341,9 @@ int frsdg_batch_create(frsdg_handle* const* handles, int32_t count, double* cons
 int frsdg_batch_step(frsdg_batch* b, void* stream);
 int frsdg_batch_run(frsdg_batch* b, int64_t max_steps, int64_t* steps, void* stream);
 /* current time of every instance (t[count]), whether it is still active and the steps it
- * has taken (active, steps: may be NULL) */
+ * has taken (active, steps: may be NULL).  With adaptive steps an instance whose step
+ * would fall below 1e-3 of its initial dt (a state whose wave speed blew up) stops:
+ * inactive with t < t_end. */
 int frsdg_batch_times(const frsdg_batch* b, double* t, int32_t* active, int64_t* steps);
 /* number of groups, and the autotuner's choice for one: order n, tile variant (0: the
  * tuned shape, 1: half its element rows), persistent CTAs of the stage launch, tiles,
