@@ -291,7 +291,7 @@ def run_reference(args, ws, rank):
     return 0
 
 
-def batched_to_t_end(device, t_end: float = 0.25) -> dict:
+def batched_to_t_end(device, t_end: float = 0.25, max_steps: int = 8000) -> dict:
     """Config 4 to t_end in FP64 and in the mixed form: time to t_end of all instances
     together, finiteness per instance and the per-instance density L2 of mixed - FP64
     (absolute and relative to the FP64 density's L2 norm)."""
@@ -303,12 +303,13 @@ def batched_to_t_end(device, t_end: float = 0.25) -> dict:
     out, finals = {}, {}
     for mixed in (False, True):
         bi = BatchedInstances(specs, device, mixed=mixed)
-        r = bi.run_persistent(t_end)
+        r = bi.run_persistent(t_end, n_steps=max_steps)
         finite = [s.status() == 0 and bool(torch.isfinite(U).all()) for _, s, U, _ in bi.items]
         finals[mixed] = [(wl.cfg, U) for wl, _, U, _ in bi.items]
         out["mixed" if mixed else "fp64"] = {
             "seconds": r.seconds, "instances": r.instances, "dofs": r.dofs, "finite_instances": int(sum(finite)),
             "steps_min_max": [min(r.steps), max(r.steps)], "graph_replays": bi.replays,
+            "stopped_before_t_end": bi.stalled,
             "stage_dof_residuals_per_s": r.stage_residuals / r.seconds, "tuning": bi.tuning}
         bi.close()
     errs, rels = [], []

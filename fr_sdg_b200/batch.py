@@ -215,7 +215,7 @@ class BatchedInstances:
         for _, s, _, _ in self.items:
             s.status()
         dts = [cfl_time_step(wl.cfg, U, wl.cfl, wl.cfl_rule) for wl, _, U, _ in self.items]
-        te = t_end if t_end is not None else float("inf")
+        te = t_end if t_end is not None else 1e300  # finite: the clocks' tolerance scales with t_end
         scales = None
         if adaptive:
             scales = []
@@ -233,6 +233,8 @@ class BatchedInstances:
         torch.cuda.synchronize(self.device)
         self.times, _, steps = db.times()
         self.replays = k  # replays of the step graph (inactive instances skip theirs)
+        # instances that stopped before t_end (adaptive step below its floor)
+        self.stalled = sum(1 for t in self.times if t < te * (1.0 - 1e-14)) if t_end is not None else 0
         self.tuning = db.tuning()
         db.close()
         finite = sum(1 for _, s, _, _ in self.items if s.status() == 0)

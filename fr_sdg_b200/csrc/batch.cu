@@ -92,6 +92,8 @@ struct Group
     BatchInst2D* d_inst = nullptr;
     int4*  d_tiles[2] = {nullptr, nullptr};
     int    ntiles[2] = {0, 0};
+    std::vector<int4> h_tiles[2];  // host copies (pruned as instances finish)
+    int    occ = 0;                // resident CTAs per SM of the chosen variant
     StabArgs* d_stab = nullptr;
     int*   d_stab_clock = nullptr;
     int4*  d_stab_tiles = nullptr;
@@ -120,6 +122,7 @@ struct frsdg_batch
     bool   tuned = false;
     cudaStream_t cs = nullptr;  // the batch's own stream (graph capture and replay)
     cudaGraphExec_t exec = nullptr;
+    int    live = 0;            // instances active when the graph was captured
     cudaEvent_t ev[2] = {nullptr, nullptr};
 };
 
@@ -293,10 +296,46 @@ int autotune(frsdg_batch* b, cudaStream_t s)
         const cudaError_t e = b->mixed ? stage_launch<float>(g.n, g.gas, g.riem, g.var, a, 0, s, &occ)
                                        : stage_launch<double>(g.n, g.gas, g.riem, g.var, a, 0, s, &occ);
         if (e != cudaSuccess) return report_cuda(e, "batch autotuner: occupancy");
+        g.occ = occ;
         g.grid = g.grid_mult == 0 ? g.ntiles[g.var]
                                   : std::min(g.ntiles[g.var], g.grid_mult * std::max(occ, 1) * b->sm_count);
     }
     b->tuned = true;
+    return FRSDG_OK;
+}
+
+// Drop the tiles of finished instances from every group's stage tile list (the
+// persistent CTAs otherwise keep walking them) and forget the captured step, which
+// holds the old counts.  Called between replays, with the batch stream idle.
+int prune(frsdg_batch* b)
+{
+    std::vector<BatchClock> clk(static_cast<size_t>(b->count));
+    cudaError_t e = cudaMemcpy(clk.data(), b->d_clock, sizeof(BatchClock) * clk.size(), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return report_cuda(e, "batch clocks");
+    int live = 0;
+    for (const BatchClock& c : clk) live += c.active ? 1 : 0;
+    for (Group& g : b->groups)
+    {
+        std::vector<int4>& ht = g.h_tiles[g.var];
+        std::vector<int4> keep;
+        keep.reserve(ht.size());
+        for (const int4& t : ht)
+            if (clk[size_t(g.members[size_t(t.x)])].active) keep.push_back(t);
+        if (keep.size() == ht.size()) continue;
+        ht.swap(keep);
+        if (!ht.empty() &&
+            (e = cudaMemcpy(g.d_tiles[g.var], ht.data(), sizeof(int4) * ht.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return report_cuda(e, "batch tiles");
+        g.ntiles[g.var] = int(ht.size());
+        g.grid = g.grid_mult == 0 ? g.ntiles[g.var]
+                                  : std::min(g.ntiles[g.var], g.grid_mult * std::max(g.occ, 1) * b->sm_count);
+    }
+    if (b->exec)
+    {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    b->live = live;
     return FRSDG_OK;
 }
 
@@ -438,6 +477,8 @@ int frsdg_batch_create(frsdg_handle* const* handles, int32_t count, double* cons
         g.nelem = elem_begin.back();
         g.ntiles[0] = int(tiles[0].size());
         g.ntiles[1] = int(tiles[1].size());
+        g.h_tiles[0] = tiles[0];
+        g.h_tiles[1] = tiles[1];
         g.nstab = int(stiles.size());
         if ((e = upload(&g.d_inst, inst)) || (e = upload(&g.d_tiles[0], tiles[0])) || (e = upload(&g.d_tiles[1], tiles[1])) ||
             (e = upload(&g.d_stab, stab)) || (e = upload(&g.d_stab_clock, stab_clock)) ||
@@ -483,8 +524,9 @@ int frsdg_batch_run(frsdg_batch* b, int64_t max_steps, int64_t* steps, void* str
         const int rc = autotune(b, b->cs);
         if (rc) return rc;
     }
-    if (!b->exec)
-    {
+    // the step of every group captured once into a CUDA graph and replayed; the graph is
+    // captured again after the tile lists lose a quarter of the live instances
+    auto capture = [&]() -> int {
         cudaGraph_t graph = nullptr;
         if ((e = cudaStreamBeginCapture(b->cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
             return report_cuda(e, "batch graph capture");
@@ -495,11 +537,18 @@ int frsdg_batch_run(frsdg_batch* b, int64_t max_steps, int64_t* steps, void* str
         e = cudaGraphInstantiate(&b->exec, graph, 0);
         cudaGraphDestroy(graph);
         if (e != cudaSuccess) return report_cuda(e, "batch graph instantiate");
-    }
+        return FRSDG_OK;
+    };
+    if (!b->live) b->live = b->count;
     int64_t k = 0;
     constexpr int kCheck = 16;  // replays between reads of the active count
     while (max_steps <= 0 || k < max_steps)
     {
+        if (!b->exec)
+        {
+            const int rc = capture();
+            if (rc) return rc;
+        }
         const int reps = max_steps > 0 ? int(std::min<int64_t>(kCheck, max_steps - k)) : kCheck;
         for (int r = 0; r < reps; ++r)
             if ((e = cudaGraphLaunch(b->exec, b->cs)) != cudaSuccess) return report_cuda(e, "batch graph launch");
@@ -508,6 +557,11 @@ int frsdg_batch_run(frsdg_batch* b, int64_t max_steps, int64_t* steps, void* str
             (e = cudaStreamSynchronize(b->cs)) != cudaSuccess)
             return report_cuda(e, "batch active count");
         if (*b->h_active == 0) break;
+        if (4 * *b->h_active < 3 * b->live)
+        {
+            const int rc = prune(b);
+            if (rc) return rc;
+        }
     }
     if (steps) *steps = k;
     if ((e = cudaEventRecord(b->ev[1], b->cs)) != cudaSuccess || (e = cudaStreamWaitEvent(s, b->ev[1], 0)) != cudaSuccess)

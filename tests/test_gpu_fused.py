@@ -37,6 +37,7 @@ def _cfg(name, stab):
     for k, v in STABS[stab].items():
         setattr(cfg, k, v)
     cfg.shock_threshold = 0.3
+    cfg.filt_cut_off = min(cfg.filt_cut_off, cfg.poly_deg - 1)  # cut-off = p gives 0/0 (rejected)
     return cfg
 
 
@@ -52,7 +53,10 @@ def _inputs(cfg, cuda):
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_fused_post_step_matches_separate_passes(name, stab, cuda):
     cfg = _cfg(name, stab)
+    # the unfused path inside the call: the post-step in 1D and with WENO alone; the
+    # limiter alone in 1D
     exact = cfg.dim == 1 or (cfg.apply_weno and not cfg.apply_filter)
+    exact_limit = cfg.dim == 1
     with FRSolver(cfg) as s:
         Us, A0, B0 = _inputs(cfg, cuda)
         kw = dict(gamma=1e-3, a=A0, alpha=1.0, b=B0, beta=1e-3)
@@ -72,9 +76,11 @@ def test_fused_post_step_matches_separate_passes(name, stab, cuda):
     assert np.all(np.isfinite(g))
     if exact:
         assert np.array_equal(g, r)
-        assert np.array_equal(got2.cpu().numpy(), ref2.cpu().numpy())
     else:
         assert rel_err(g, r) <= 1e-13, f"{name} {stab}: post-step rel err {rel_err(g, r):.3e}"
+    if exact_limit:
+        assert np.array_equal(got2.cpu().numpy(), ref2.cpu().numpy())
+    else:
         e2 = rel_err(got2.cpu().numpy(), ref2.cpu().numpy())
         assert e2 <= 1e-13, f"{name} {stab}: limiter rel err {e2:.3e}"
     if cfg.pp_limit:
