@@ -370,12 +370,13 @@ int frsdg_batch_create(frsdg_handle* const* handles, int32_t count, double* cons
     if ((e = cudaGetDevice(&b->device)) != cudaSuccess) return fail_cuda(e, "cudaGetDevice");
     if ((e = cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, b->device)) != cudaSuccess)
         return fail_cuda(e, "device attribute");
-    // groups by (order, gas law, flux, correction)
-    std::map<std::tuple<int, int, int, double>, int> gid;
+    // groups by (order, gas law, flux, correction, filter): the group's operators
+    std::map<std::tuple<int, int, int, double, int, int, double>, int> gid;
     for (int i = 0; i < count; ++i)
     {
         const frsdg_handle* h = handles[i];
-        const auto key = std::make_tuple(h->n, h->cfg.gas_law, h->cfg.riemann, h->cfg.radau_corr);
+        const auto key = std::make_tuple(h->n, h->cfg.gas_law, h->cfg.riemann, h->cfg.radau_corr, h->cfg.filt_cut_off,
+                                         h->cfg.filt_strength, h->cfg.filt_alpha);
         auto it = gid.find(key);
         if (it == gid.end())
         {
@@ -403,7 +404,6 @@ int frsdg_batch_create(frsdg_handle* const* handles, int32_t count, double* cons
     {
         const frsdg_handle* h = handles[i];
         PostArgs& p = post[size_t(i)];
-        for (int q = 0; q < h->n * h->n; ++q) p.F[q] = h->st.F[q];
         for (int q = 0; q < h->n; ++q) p.w[q] = h->re.w[q];
         p.pp_eps = h->cfg.pp_eps;
         p.detJ = nullptr;  // affine

@@ -504,7 +504,7 @@ int frsdg_create(const frsdg_config* cfg, frsdg_handle** out)
         s.theta = cfg->shock_theta;
         s.threshold = cfg->shock_threshold;
         const auto F = build_filter_matrix(h->re, cfg->filt_cut_off, cfg->filt_strength, cfg->filt_alpha);
-        for (int q = 0; q < n * n; ++q) { s.F[q] = F[q]; s.D[q] = h->re.D[q]; }
+        for (int q = 0; q < n * n; ++q) { s.F[q] = F[q]; s.D[q] = h->re.D[q]; h->a2.ops.F[q] = F[q]; }
         for (int q = 0; q < n; ++q) s.w[q] = h->re.w[q];
         if (cfg->apply_weno && !cfg->apply_filter)
         {
@@ -521,7 +521,6 @@ int frsdg_create(const frsdg_config* cfg, frsdg_handle** out)
     if (cfg->dim == 2)
     {
         PostArgs pa{};
-        for (int q = 0; q < n * n; ++q) pa.F[q] = h->st.F[q];
         for (int q = 0; q < n; ++q) pa.w[q] = h->re.w[q];
         pa.pp_eps = cfg->pp_eps;
         pa.detJ = h->d_detJ;

@@ -58,6 +58,7 @@ struct Ops
     float  Df[kMaxN * kMaxN];  // FP32 copies for the single-precision residual
     float  dLf[kMaxN];
     float  dRf[kMaxN];
+    double F[kMaxN * kMaxN];   // spectral filter matrix (the stage epilogue's post-step)
 };
 
 // Operator entries in the arithmetic type T of a residual instantiation.
@@ -88,8 +89,7 @@ enum : int
 };
 struct PostArgs
 {
-    double F[kMaxN * kMaxN];   // filter matrix, row-major (StabArgs::F)
-    double w[kMaxN];           // GLL weights
+    double w[kMaxN];           // GLL weights (the filter matrix is Ops::F)
     double pp_eps;             // the limiter's floor (cfg.pp_eps)
     const double* detJ;        // per-node detJ [global element][node] (curved meshes), or null
     unsigned long long* amax;  // POST_AMAX: atomicMax target (bits of a positive double)

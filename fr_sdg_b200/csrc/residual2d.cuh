@@ -419,8 +419,8 @@ __device__ __forceinline__ void face_jumps(const Fr2dArgs& a, int i0, int j0, bo
 // along the element's rows and along its columns), the positivity limiter and the
 // wave-speed maximum act on each element in shared memory, then the tile is stored.
 template <class T, int N, int GAS>
-__device__ __forceinline__ void stage_epilogue(const Fr2dArgs& a, int i0, int j0, int txe, int tye, double* sO,
-                                               unsigned char* smem_raw)
+__device__ __forceinline__ void stage_epilogue(const Fr2dArgs& a, const Ops& ops, int i0, int j0, int txe, int tye,
+                                               double* sO, unsigned char* smem_raw)
 {
     constexpr int TX = T::TX, TE = T::TE, BT = T::BT, NN = N * N, ND = 4 * NN;
     static_assert(BT % 32 == 0, "whole warps");
@@ -446,7 +446,7 @@ __device__ __forceinline__ void stage_epilogue(const Fr2dArgs& a, int i0, int j0
                 {
                     double acc = 0.0;
 #pragma unroll
-                    for (int c = 0; c < N; ++c) acc += __ldg(&P.F[r * N + c]) * cv[c];
+                    for (int c = 0; c < N; ++c) acc += ops.F[r * N + c] * cv[c];
                     double& d = sY[e * ND + (dir == 0 ? m * N + r : r * N + m) * 4 + eq];
                     d = dir == 0 ? acc : 0.5 * (d + acc);
                 }
@@ -853,7 +853,7 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
         if (post)
         {
             __syncthreads();
-            stage_epilogue<T, N, GAS>(a, i0, j0, txe, tye, sO, smem_raw);
+            stage_epilogue<T, N, GAS>(a, ops, i0, j0, txe, tye, sO, smem_raw);
         }
     }
 }
