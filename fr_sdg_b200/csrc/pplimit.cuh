@@ -13,6 +13,7 @@
 // It has no counterpart in the reference.  The argument type PA provides gas_law, gas,
 // eps0, w[] (GLL weights) and detJ (per-node Jacobian determinants, or null).
 #pragma once
+#include "device_math.cuh"
 #include "frsdg_internal.hpp"
 
 namespace frsdg
@@ -64,6 +65,34 @@ template <class PA> __device__ __forceinline__ double node_wave_speed(const PA& 
     return sqrt(vx * vx + vy * vy) + sqrt(fmax(c2, 0.0));
 }
 
+// The same quantities with reciprocals (device_math.cuh: within 2 ulp of the
+// quotients): the screen that lets admissible elements skip the limiter, and the wave
+// speed of the adaptive time step, where rounding is immaterial.
+template <class PA> __device__ __forceinline__ double pp_pressure_fast(const PA& a, const double* u)
+{
+    const double ir = s_rcp(u[0]);
+    const double rho_e = u[3] - 0.5 * (u[1] * u[1] + u[2] * u[2]) * ir;  // rho e
+    if (a.gas_law == FRSDG_GAS_IDEAL) return (a.gas.gamma - 1.0) * rho_e;
+    const double rho = u[0];
+    return ((a.gas.gamma - 1.0) * (rho_e + a.gas.a * rho * rho)) * s_rcp(1.0 - a.gas.b * rho) - a.gas.a * rho * rho;
+}
+template <class PA> __device__ __forceinline__ double node_wave_speed_fast(const PA& a, const double* u)
+{
+    const double rho = u[0], ir = s_rcp(rho);
+    const double vx = u[1] * ir, vy = u[2] * ir;
+    const double v2 = vx * vx + vy * vy;
+    const double e = u[3] * ir - 0.5 * v2;
+    double c2;
+    if (a.gas_law == FRSDG_GAS_IDEAL) c2 = a.gas.gamma * (a.gas.gamma - 1.0) * e;
+    else
+    {
+        const double cov = 1.0 - a.gas.b * rho, gm1 = a.gas.gamma - 1.0, ic2 = s_rcp(cov * cov);
+        c2 = (a.gas.gamma * gm1 * (e + a.gas.a * rho)) * ic2 + (gm1 * a.gas.a * rho * (2.0 - a.gas.b * rho)) * ic2 -
+             2.0 * a.gas.a * rho;
+    }
+    return s_sqrt(v2) + s_sqrt(fmax(c2, 0.0));
+}
+
 template <int NV, class PA>
 __device__ __forceinline__ double pp_segment_root(const PA& a, const double* ub, const double* uq, double eps)
 {
@@ -103,19 +132,54 @@ __device__ __forceinline__ void pp_element2d(const PA& a, double* base, float* b
     const int lane = threadIdx.x & 31;
     double u[R][4], W[R];
     double wsum = 0.0, ub[4] = {0.0, 0.0, 0.0, 0.0};
+    // screen: an element whose nodes all have density and pressure above eps0 is left
+    // as it is (eps <= eps0), so it needs no cell average (nodes within 1e-10 of the
+    // floor take the exact path)
+    bool clear = true;
 #pragma unroll
     for (int r = 0; r < R; ++r)
     {
         const int q = lane + 32 * r;
-        W[r] = 0.0;
         u[r][0] = u[r][1] = u[r][2] = u[r][3] = 0.0;
         if (q < NQ)
         {
             const double2 x0 = *reinterpret_cast<const double2*>(base + q * 4);
             const double2 x1 = *reinterpret_cast<const double2*>(base + q * 4 + 2);
             u[r][0] = x0.x; u[r][1] = x0.y; u[r][2] = x1.x; u[r][3] = x1.y;
-            W[r] = a.w[q % N] * a.w[q / N] * (a.detJ ? __ldg(a.detJ + e_glob * NQ + q) : 1.0);
+            const double thr = a.eps0 * (1.0 + 1e-10);
+            clear = clear && u[r][0] > thr && pp_pressure_fast(a, u[r]) > thr;
         }
+    }
+    if (__all_sync(0xffffffffu, clear || !limit))
+    {
+        if (amax)
+        {
+            double w = 0.0;
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (lane + 32 * r < NQ) w = fmax(w, node_wave_speed_fast(a, u[r]));
+            w = -pp_warp_min(-w);
+            if (lane == 0 && w > 0.0 && w < 1e300)
+                atomicMax(amax, static_cast<unsigned long long>(__double_as_longlong(w)));
+        }
+        if (refresh32 && base32)
+        {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+            {
+                const int q = lane + 32 * r;
+                if (q < NQ)
+                    *reinterpret_cast<float4*>(base32 + q * 4) =
+                        make_float4(float(u[r][0]), float(u[r][1]), float(u[r][2]), float(u[r][3]));
+            }
+        }
+        return;
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+    {
+        const int q = lane + 32 * r;
+        W[r] = q < NQ ? a.w[q % N] * a.w[q / N] * (a.detJ ? __ldg(a.detJ + e_glob * NQ + q) : 1.0) : 0.0;
         wsum += W[r];
 #pragma unroll
         for (int c = 0; c < 4; ++c) ub[c] += W[r] * u[r][c];
@@ -161,7 +225,7 @@ __device__ __forceinline__ void pp_element2d(const PA& a, double* base, float* b
         double w = 0.0;
 #pragma unroll
         for (int r = 0; r < R; ++r)
-            if (lane + 32 * r < NQ) w = fmax(w, node_wave_speed(a, u[r]));
+            if (lane + 32 * r < NQ) w = fmax(w, node_wave_speed_fast(a, u[r]));
         w = -pp_warp_min(-w);
         if (lane == 0 && w > 0.0 && w < 1e300) atomicMax(amax, static_cast<unsigned long long>(__double_as_longlong(w)));
     }
