@@ -426,6 +426,9 @@ __device__ __forceinline__ void stage_epilogue(const Fr2dArgs& a, const Ops& ops
     static_assert(BT % 32 == 0, "whole warps");
     const int tid = threadIdx.x;
     const PostArgs& P = *a.pa;
+    const bool filter = (a.post & POST_FILTER) != 0;
+    __shared__ int s_flag[TE];  // elements the limiter changed (their stored values are stale)
+    for (int e = tid; e < TE; e += BT) s_flag[e] = 0;
     double* sX = sO;
     if (a.post & POST_FILTER)
     {
@@ -457,22 +460,57 @@ __device__ __forceinline__ void stage_epilogue(const Fr2dArgs& a, const Ops& ops
     }
     if (a.post & (POST_PP | POST_AMAX))
     {
+        // screen every node of the tile at once (pp_element2d's test: density and
+        // pressure above the floor leave the element as it is); only the elements with
+        // a node below it go through the limiter, one warp each.  Clear elements give
+        // their wave speeds here, limited ones after limiting.
         const PPView v{GAS == 0 ? FRSDG_GAS_IDEAL : FRSDG_GAS_VDW, a.gas, P.pp_eps, P.w, P.detJ};
-        unsigned long long* amax = (a.post & POST_AMAX) ? P.amax : nullptr;
-        for (int e = tid / 32; e < TE; e += BT / 32)
+        const bool limit = (a.post & POST_PP) != 0, want_amax = (a.post & POST_AMAX) != 0;
+        __shared__ unsigned long long s_amax;
+        if (tid == 0) s_amax = 0ull;
+        __syncthreads();
+        const double thr = v.eps0 * (1.0 + 1e-10);
+        double w = 0.0;
+        for (int q = tid; q < TE * NN; q += BT)
         {
-            const int tx = e % TX, ty = e / TX;
-            if (tx >= txe || ty >= tye) continue;  // uniform across the warp
-            const int64_t e_glob = int64_t(j0 + ty + a.row_base) * a.Nx + (i0 + tx);
-            pp_element2d<N>(v, sX + e * ND, nullptr, e_glob, (a.post & POST_PP) != 0, false, amax);
+            const int e = q / NN;
+            if (e % TX >= txe || e / TX >= tye) continue;
+            const double2 x0 = *reinterpret_cast<const double2*>(sX + q * 4);
+            const double2 x1 = *reinterpret_cast<const double2*>(sX + q * 4 + 2);
+            const double u[4] = {x0.x, x0.y, x1.x, x1.y};
+            if (limit && !(u[0] > thr && pp_pressure_fast(v, u) > thr)) s_flag[e] = 1;
+            else if (want_amax) w = fmax(w, node_wave_speed_fast(v, u));
+        }
+        if (want_amax)
+        {
+            w = -pp_warp_min(-w);
+            if ((tid & 31) == 0 && w > 0.0 && w < 1e300)
+                atomicMax(&s_amax, static_cast<unsigned long long>(__double_as_longlong(w)));
         }
         __syncthreads();
+        if (limit)
+        {
+            unsigned long long* amax = want_amax ? &s_amax : nullptr;
+            for (int e = tid / 32; e < TE; e += BT / 32)
+            {
+                const int tx = e % TX, ty = e / TX;
+                if (tx >= txe || ty >= tye || !s_flag[e]) continue;  // uniform across the warp
+                const int64_t e_glob = int64_t(j0 + ty + a.row_base) * a.Nx + (i0 + tx);
+                pp_element2d<N>(v, sX + e * ND, nullptr, e_glob, true, false, amax);
+            }
+            __syncthreads();
+        }
+        if (want_amax && tid == 0 && s_amax) atomicMax(P.amax, s_amax);
     }
+    // store: the filtered tile, or (values already stored by the row pass) the
+    // elements the limiter changed
+    if (!filter && !(a.post & POST_PP)) return;
+    if (!filter) __syncthreads();  // s_flag complete (the limiter's own barrier may be skipped)
     double* out = static_cast<double*>(a.out);
     for (int q = tid; q < TE * (ND / 2); q += BT)
     {
         const int e = q / (ND / 2), k = q % (ND / 2), tx = e % TX, ty = e / TX;
-        if (tx >= txe || ty >= tye) continue;
+        if (tx >= txe || ty >= tye || !(filter || s_flag[e])) continue;
         reinterpret_cast<double2*>(out + (int64_t(j0 + ty) * a.Nx + (i0 + tx)) * ND)[k] =
             reinterpret_cast<const double2*>(sX + e * ND)[k];
     }
@@ -841,7 +879,13 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
             else if (a.out_f32)
                 reinterpret_cast<float*>(a.out)[gidx] = static_cast<float>(s_re(R));
             else if (post)
-                sO[e * ND + (l * N + k) * 4 + eq] = stage_value(a.st, gidx, s_re(R));
+            {
+                // the epilogue's input; without the filter the value is also final
+                // unless the limiter changes its element, so it is stored now
+                const double v = stage_value(a.st, gidx, s_re(R));
+                sO[e * ND + (l * N + k) * 4 + eq] = v;
+                if (!(a.post & POST_FILTER)) out[gidx] = v;
+            }
             else
             {
                 store_residual(a.mode, a.W, a.st, out, gidx, s_re(R));
