@@ -419,7 +419,7 @@ __device__ __forceinline__ void face_jumps(const Fr2dArgs& a, int i0, int j0, bo
 // along the element's rows and along its columns), the positivity limiter and the
 // wave-speed maximum act on each element in shared memory, then the tile is stored.
 template <class T, int N, int GAS>
-__device__ __forceinline__ void stage_epilogue(const Fr2dArgs& a, const Ops& ops, int i0, int j0, int txe, int tye,
+__device__ __noinline__ void stage_epilogue(const Fr2dArgs& a, const Ops& ops, int i0, int j0, int txe, int tye,
                                                double* sO, unsigned char* smem_raw)
 {
     constexpr int TX = T::TX, TE = T::TE, BT = T::BT, NN = N * N, ND = 4 * NN;
@@ -550,7 +550,8 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
     S* sRec = sm + T::oRec;
     S* sDel = sm + T::oDel;
     // stage epilogue: the tile's stage outputs (Tile2D::POST_IN_REC)
-    const bool post = POST && !T::JVP && a.mode == MODE_STAGE && a.post != 0;
+    // (POST instantiations run only stage launches: the launcher and the batch kernel)
+    constexpr bool post = POST && !T::JVP;
     double* sO = reinterpret_cast<double*>(smem_raw + (T::POST_IN_REC ? T::oRec * sizeof(S) : T::bytes));
     double* sSeed = reinterpret_cast<double*>(smem_raw + size_t(T::nS) * sizeof(S));
 
@@ -892,13 +893,10 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
             }
         }
     }
-    if constexpr (POST && !T::JVP)
+    if constexpr (post)
     {
-        if (post)
-        {
-            __syncthreads();
-            stage_epilogue<T, N, GAS>(a, ops, i0, j0, txe, tye, sO, smem_raw);
-        }
+        __syncthreads();
+        stage_epilogue<T, N, GAS>(a, ops, i0, j0, txe, tye, sO, smem_raw);
     }
 }
 
