@@ -436,6 +436,18 @@ def run_ours(args, ws, rank, local):
         mixed = {"fp32_residual_ms": mms, "fp32_dof_residuals_per_s": ws * dofs / (mms / 1e3),
                  "speedup_vs_fp64": (elapsed_ms / args.steps) / mms,
                  "fp64_stage_ms": sms, "mixed_stage_ms": xms, "mixed_stage_speedup": sms / xms}
+        # the FP32 residual with its derivative contractions on the tensor cores (tcgen05,
+        # split TF32, cfg.mixed_tc = 1; p = 4 and 5 only)
+        if wl.cfg.poly_deg in (4, 5):
+            saved_tc = wl.cfg.mixed_tc
+            wl.cfg.mixed_tc = 1
+            with FRSolver(wl.cfg) as ts:
+                tms = event_ms(lambda: ts.residual_kernel_f32(0.0, U32, F32))
+                txms = event_ms(lambda: ts.rk_stage_mixed(0.0, U, out, gamma=1e-3, a=U, alpha=1.0))
+            wl.cfg.mixed_tc = saved_tc
+            mixed["tensor_cores"] = {"fp32_residual_ms": tms, "fp32_dof_residuals_per_s": ws * dofs / (tms / 1e3),
+                                     "mixed_stage_ms": txms,
+                                     "path": "tcgen05.mma kind::tf32, operands split hi + lo, FP32 accumulation"}
         # the last SSP-RK3 stage with the post-step (spectral filter + positivity limiter)
         # in its epilogue against the stage and the post-step as two launches
         if blk is None:

@@ -49,7 +49,7 @@ class frsdg_config(C.Structure):
         ("shock_theta", C.c_double), ("shock_threshold", C.c_double),
         ("cond_sys", C.c_int32), ("jvp_exact_bc", C.c_int32),
         ("csd_eps", C.c_double),
-        ("pp_limit", C.c_int32), ("pad1_", C.c_int32), ("pp_eps", C.c_double),
+        ("pp_limit", C.c_int32), ("mixed_tc", C.c_int32), ("pp_eps", C.c_double),
     ]
 
 
@@ -96,6 +96,7 @@ SIGNATURES = {
                                      C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "frsdg_batch_destroy": (C.c_int, [_P]),
     "frsdg_device_math": (C.c_int, [C.c_int32, _P, _P, C.c_int64, _P]),
+    "frsdg_tc_lines": (C.c_int, [C.c_int32, _P, _P, _P, C.c_int64, _P]),
     "frsdg_petsc_vec_record_bytes": (C.c_int, [C.c_int64, C.c_int32, C.POINTER(C.c_int64)]),
     "frsdg_petsc_vec_pack": (C.c_int, [_P, C.c_int64, C.c_int32, _P, _P]),
     "frsdg_reference_element": (C.c_int, [C.c_int32, _D, _P, _P, _P, _P, _P]),

@@ -215,6 +215,7 @@ int frsdg_config_default(frsdg_config* c)
     c->cond_sys = 0;
     c->csd_eps = 1e-7;
     c->pp_limit = 0;
+    c->mixed_tc = 0;
     c->pp_eps = 1e-13;
     return FRSDG_OK;
 }
@@ -335,6 +336,7 @@ int frsdg_create(const frsdg_config* cfg, frsdg_handle** out)
         a.bad = h->d_bad;
         a.nd = 4 * n * n;
         a.exact_bc = cfg->jvp_exact_bc;
+        a.tc = cfg->mixed_tc ? 1 : 0;
         a.jac_cmode = ((per_x && (Nx & 1)) || (per_y && (Ny & 1))) ? 1 : 0;
         for (int d = 0; d < 4; ++d)
         {
@@ -1115,6 +1117,25 @@ int frsdg_device_math(int32_t op, const double* x, double* y, int64_t n, void* s
     const cudaError_t e = launch_device_math(op, x, y, n, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_fail(e, "device-math launch");
     return FRSDG_OK;
+}
+
+int frsdg_tc_lines(int32_t n, const float* v, const double* D, float* out, int64_t lines, void* stream)
+{
+    if (n < 2 || n > 8 || lines < 0 || (lines > 0 && (!v || !D || !out))) return fail(FRSDG_ERR_ARG, "bad argument");
+    if (lines == 0) return FRSDG_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int* err = nullptr;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&err), sizeof(int), s);
+    if (e != cudaSuccess) return cuda_fail(e, "tensor-core flag allocation");
+    int h_err = 0;
+    if ((e = cudaMemsetAsync(err, 0, sizeof(int), s)) == cudaSuccess &&
+        (e = launch_tc_lines(n, v, D, out, lines, err, s)) == cudaSuccess)
+        e = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    const cudaError_t e2 = cudaFreeAsync(err, s);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "tensor-core line contraction");
+    return h_err ? fail(FRSDG_ERR_CUDA, "tensor-core completion wait gave up") : FRSDG_OK;
 }
 
 int frsdg_status(frsdg_handle* h, int64_t* bad_nodes)

@@ -123,6 +123,7 @@ struct Fr2dArgs
     int    jac_cmode;  // MODE_JAC colouring: 0 checkerboard, 1 three-colour cycles (odd periodic),
                        // 2 distance-2 colouring (i + 2 j) mod 5 for all five blocks of an element row
     int    in_f64;     // FP32 instantiation: U is an FP64 state, node primitives recovered in FP64
+    int    tc;         // FP32 instantiation at n = 5, 6: derivative contractions on the tensor cores
     Ops    ops;
     // (after the operators: a batch launch sets these per stage, not per instance)
     int    post;       // MODE_STAGE: element-local post-processing of the stage output (POST_*)

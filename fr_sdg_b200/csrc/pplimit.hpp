@@ -46,5 +46,7 @@ cudaError_t launch_check_density(int dim, int n, int64_t nelem, const double* U,
                                  cudaStream_t s);
 // y = s_rcp(x) (op 0) or s_sqrt(x) (op 1), elementwise
 cudaError_t launch_device_math(int op, const double* x, double* y, int64_t n, cudaStream_t s);
+// tc.cu: the split-precision tensor-core line contraction on its own (validation)
+cudaError_t launch_tc_lines(int n, const float* v, const double* D, float* out, int64_t L, int* err, cudaStream_t s);
 
 } // namespace frsdg

@@ -23,6 +23,7 @@
 #include "frsdg_internal.hpp"
 #include "physics.cuh"
 #include "pplimit.cuh"
+#include "tc_sm100.cuh"
 
 namespace frsdg
 {
@@ -75,7 +76,10 @@ __host__ __device__ constexpr int reg_cap(int n, int words, bool f32, int bt)
 
 // VAR selects the tile: 0 the tuned shape of tile_x/tile_y, 1 the same tile with half
 // the element rows (fewer elements per CTA; a candidate of the batch autotuner).
-template <class S, int N, int GEO, int VAR = 0> struct Tile2D
+// TC: the FP32 face tiles (n = 5, 6) with the derivative contractions on the tensor
+// cores (tc_sm100.cuh); their operands and barrier take a region at the front of the
+// shared memory, the tile's usual layout follows it.
+template <class S, int N, int GEO, int VAR = 0, bool TC = false> struct Tile2D
 {
     static constexpr int W  = scalar_traits<S>::words;
     static constexpr bool F32 = sizeof(S) == 4;
@@ -85,7 +89,12 @@ template <class S, int N, int GEO, int VAR = 0> struct Tile2D
     static constexpr int TE = TX * TY;
     static constexpr bool JVP = scalar_traits<S>::words == 2;
     static constexpr int BT = block_threads(N, W, F32, TX, TY);
-    static constexpr int MAXREG = reg_cap(N, W, F32, BT) > 255 ? 255 : reg_cap(N, W, F32, BT);
+    // tensor-core tiles: shared memory admits four or five CTAs per SM, so 80 registers
+#ifdef FRSDG_TC_MAXREG
+    static constexpr int MAXREG = TC ? FRSDG_TC_MAXREG : reg_cap(N, W, F32, BT) > 255 ? 255 : reg_cap(N, W, F32, BT);
+#else
+    static constexpr int MAXREG = TC ? 80 : reg_cap(N, W, F32, BT) > 255 ? 255 : reg_cap(N, W, F32, BT);
+#endif
     static constexpr int NB = 4 * N - 4;  // boundary nodes per element
     static constexpr int NREC_E = TE * NB;
     static constexpr int NHALO  = 2 * TY * N + 2 * TX * N;
@@ -106,7 +115,25 @@ template <class S, int N, int GEO, int VAR = 0> struct Tile2D
     // after P3)
     static constexpr size_t post_bytes = size_t(TE) * 4 * NN * sizeof(double);
     static constexpr bool POST_IN_REC = size_t(RF_N) * NREC * sizeof(S) >= post_bytes;
-    static constexpr size_t bytes_post = POST_IN_REC ? bytes : bytes + post_bytes;
+    // tensor-core region: [barrier, TMEM base | A_hi | A_lo | B_hi | B_lo].  The
+    // contractions run in two passes through one operand buffer: pass 0 the xi-lines
+    // (of F; curved meshes also of G), pass 1 the eta-lines (of G; curved also of F),
+    // LSP sets of LINES lines per pass, two 128-line MMA tiles per set.  The second tile
+    // of a set reads up to 256 - LINES rows past the set's end: into the next set, or
+    // past A_lo into B and the tile region, all inside the CTA's shared memory, and only
+    // into accumulator rows nobody reads.  The region is padded so that TMEM columns per
+    // byte of shared memory stay below 512 per 228 KB: every mix of these CTAs that fits
+    // an SM's shared memory finds its columns free.
+    static constexpr int LSP = GEO == GEO_CURVED ? 2 : 1;
+    static constexpr int LINES = TE * 4 * N;
+    static constexpr int LP = (LINES + 7) / 8 * 8;
+    static constexpr int TC_COLS = 2 * LSP * 2 * tc::kCols;  // TMEM columns (a power of two)
+    static constexpr size_t tc_a_bytes = size_t(LSP) * LP * tc::kRowBytes;
+    static constexpr size_t tc_raw = 128 + 2 * tc_a_bytes + 2 * tc::kBBytes;
+    static constexpr size_t tc_min = size_t(TC_COLS) * (228 * 1024 / 512) - 1024 - bytes;
+    static constexpr size_t tc_bytes = !TC ? 0 : (tc_raw >= tc_min || tc_min > 1u << 30 ? tc_raw : (tc_min + 127) / 128 * 128);
+    static constexpr size_t bytes_post = tc_bytes + (POST_IN_REC ? bytes : bytes + post_bytes);
+    static constexpr size_t bytes_launch = tc_bytes + bytes;
     // index of boundary node (k, l) among an element's NB boundary nodes:
     // bottom row, top row, then the interior of the left and right columns
     __host__ __device__ static constexpr int bidx(int k, int l)
@@ -536,14 +563,21 @@ template <class S, int N> __device__ __forceinline__ void center_line(S (&v)[N])
 
 // POST: the instantiation with the stage epilogue (Fr2dArgs::post); the others carry no
 // epilogue code, which would otherwise cost the main path registers.
-template <class S, int N, int GAS, int RIEM, int GEO, int VAR, bool POST = false>
+template <class S, int N, int GAS, int RIEM, int GEO, int VAR, bool POST = false, bool TC = false>
 __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int bx, int by, unsigned char* smem_raw)
 {
-    using T = Tile2D<S, N, GEO, VAR>;
+    using T = Tile2D<S, N, GEO, VAR, TC>;
     constexpr int TX = T::TX, TY = T::TY, NN = T::NN, TE = T::TE, BT = T::BT, NREC = T::NREC;
     using R_t = typename scalar_traits<S>::real;
     constexpr int ND = 4 * NN;
-    S* sm   = reinterpret_cast<S*>(smem_raw);
+    static_assert(!TC || (T::F32 && (N == 5 || N == 6)), "tensor-core contractions: FP32 face tiles at n = 5, 6");
+    static_assert(!TC || (T::LINES <= BT && BT <= 2 * tc::kTileLines), "one line of each set per thread");
+    // every CTA of every mix of these kernels that fits on an SM (228 KB of shared memory)
+    // finds its TMEM columns free: columns per byte of shared memory stay below 512 / 228 KB
+    static_assert(!TC || size_t(T::TC_COLS) * (228 * 1024) <= size_t(512) * (T::bytes_launch + 1024),
+                  "TMEM columns per CTA against shared memory per CTA");
+    unsigned char* base = smem_raw + T::tc_bytes;  // the tile's layout (tensor-core region first)
+    S* sm   = reinterpret_cast<S*>(base);
     S* sF   = sm + T::oF;
     S* sG   = sm + T::oG;
     S* sC   = sm + T::oC;
@@ -552,14 +586,30 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
     // stage epilogue: the tile's stage outputs (Tile2D::POST_IN_REC)
     // (POST instantiations run only stage launches: the launcher and the batch kernel)
     constexpr bool post = POST && !T::JVP;
-    double* sO = reinterpret_cast<double*>(smem_raw + (T::POST_IN_REC ? T::oRec * sizeof(S) : T::bytes));
-    double* sSeed = reinterpret_cast<double*>(smem_raw + size_t(T::nS) * sizeof(S));
+    double* sO = reinterpret_cast<double*>(base + (T::POST_IN_REC ? T::oRec * sizeof(S) : T::bytes));
+    double* sSeed = reinterpret_cast<double*>(base + size_t(T::nS) * sizeof(S));
+    // tensor-core region
+    uint64_t* tc_bar = reinterpret_cast<uint64_t*>(smem_raw);
+    uint32_t* tc_tmem = reinterpret_cast<uint32_t*>(smem_raw + 8);
+    unsigned char* tc_ahi = smem_raw + 128;
+    unsigned char* tc_alo = tc_ahi + T::tc_a_bytes;
+    unsigned char* tc_bhi = tc_alo + T::tc_a_bytes;
+    unsigned char* tc_blo = tc_bhi + tc::kBBytes;
 
     const int tid = threadIdx.x;
     const int Nx = a.Nx, Ny = a.Ny;
     const int i0 = bx * TX, j0 = by * TY + a.row_begin;
     const int txe = min(TX, Nx - i0), tye = min(TY, a.row_end - j0);
     const GasParams g = a.gas;
+
+    if constexpr (TC)
+    {
+        // TMEM for the accumulators (warp 0), the MMA-completion barrier, and the split
+        // differentiation matrix as the B operand (16 rows)
+        if (tid < 32) tc::tmem_alloc(tc_tmem, T::TC_COLS);
+        else if (tid == 32) tc::mbar_init(tc_bar, 1);
+        else if (tid >= 64 && tid < 64 + tc::kCols) tc::pack_matrix_row<N>(tc_bhi, tc_blo, tid - 64, ops.D);
+    }
 
     if constexpr (!T::JVP)
     {
@@ -696,7 +746,63 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
 #pragma unroll
         for (int fld = 0; fld < RF_N; ++fld) sRec[fld * NREC + hrec] = rec[fld];
     }
+    if constexpr (TC)
+    {
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+    }
     __syncthreads();
+    uint32_t tmem = 0;
+    // tensor cores: the flux lines of one pass, each minus its first value (center_line),
+    // split into TF32 high and low parts as the A operands of the shared buffer, by the
+    // threads first, first + stride, ...; and the MMAs of a pass, issued by one thread
+    auto tc_pack = [&](int pass, int first, int stride) {
+        if constexpr (TC)
+        {
+            for (int q = first; q < T::LSP * T::LINES; q += stride)
+            {
+                const int set = q / T::LINES, t = q % T::LINES;
+                const int eq = t % 4, l = (t / 4) % N, e = t / (4 * N);
+                const bool xi = pass == 0;
+                const S* src = ((set == 0) == xi ? sF : sG) + (e * 4 + eq) * NN + (xi ? l * N : l);
+                S v[N];
+#pragma unroll
+                for (int m = 0; m < N; ++m) v[m] = src[xi ? m : m * N];
+                center_line<S, N>(v);
+                tc::pack_line<N>(tc_ahi, tc_alo, set * T::LP + t, v);
+            }
+        }
+    };
+    auto tc_issue = [&](int pass) {
+        if constexpr (TC)
+        {
+            const uint32_t ah = tc::smem_u32(tc_ahi), al = tc::smem_u32(tc_alo);
+            const uint32_t bh = tc::smem_u32(tc_bhi), bl = tc::smem_u32(tc_blo);
+#pragma unroll
+            for (int set = 0; set < T::LSP; ++set)
+            {
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+                {
+                    const uint32_t off = uint32_t(set * T::LP + q * tc::kTileLines) * tc::kRowBytes;
+                    tc::split_product(tmem, uint32_t((pass * T::LSP + set) * 2 + q) * tc::kCols, ah + off, al + off,
+                                      bh, bl);
+                }
+            }
+            tc::mma_commit(tc_bar);
+        }
+    };
+    if constexpr (TC)
+    {
+        // pass 0 (xi-lines) by every thread; its MMAs run while the face phase solves its
+        // Riemann problems, and the column warps pack and issue pass 1 once they are done
+        tc::fence_after_sync();
+        tmem = *tc_tmem;
+        tc_pack(0, tid, BT);
+        tc::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) tc_issue(0);
+    }
 
     // ---- P2: face points and element columns.  When the block has threads to
     // spare, each face thread solves one face point (x-faces, then y-faces, on
@@ -779,9 +885,24 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
                 face_jumps<S, N, GEO, false, T>(a, i0, j0, true, sd, Fs, sF, sG, sDel);
             }
         }
-        else
+        else if constexpr (!TC)
         {
             for (int c = tid - PX - PY; c < NCOL; c += BT - PX - PY) column(c);
+        }
+        else
+        {
+            // the column warps: once pass 0's MMAs have read the buffer (barrier phase 0),
+            // pack pass 1 (eta-lines) into it and issue its MMAs (phase 1)
+            constexpr int NCW = BT - PX - PY;
+            static_assert(NCW % 32 == 0 && NCW > 0, "whole column warps");
+            if (!tc::mbar_wait(tc_bar, 0, 1 << 20) && a.bad) atomicAdd(a.bad, 1ull << 32);
+            tc_pack(1, tid - PX - PY, NCW);
+            tc::fence_async_smem();
+            if constexpr (NCW == 32)
+                __syncwarp();
+            else
+                asm volatile("bar.sync 1, %0;" ::"n"(NCW) : "memory");
+            if (tid == PX + PY) tc_issue(1);
         }
     }
     else
@@ -807,6 +928,44 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
         }
     }
     __syncthreads();
+    // tensor cores: the eta-derivatives of line t (element column k = l of set 1, and of
+    // set 3 on curved meshes) go to sC at the nodes (m, l), as the column pass stores them
+    float xiF[8], xiG[8];
+    if constexpr (TC)
+    {
+        static_assert(UNPAIR, "the column warps pack the second pass");
+        // phase 1: pass 1's MMAs (issued after phase 0 completed) are done
+        const bool done = tc::mbar_wait(tc_bar, 1, 1 << 20);
+        tc::fence_after_sync();
+        if (!done && tid == 0 && a.bad) atomicAdd(a.bad, 1ull << 32);  // flagged, never waited on again
+        const int t = tid, eq = t % 4, l = (t / 4) % N, e = t / (4 * N);
+        const uint32_t tile = uint32_t(t / tc::kTileLines);
+        constexpr uint32_t P1 = 2 * T::LSP * tc::kCols;  // first column of pass 1
+        float dG[8], dF[8];
+        tc::load8(tmem, P1 + tile * tc::kCols, dG);
+        if constexpr (GEO == GEO_CURVED) tc::load8(tmem, P1 + (2 + tile) * tc::kCols, dF);
+        tc::load8(tmem, tile * tc::kCols, xiF);
+        if constexpr (GEO == GEO_CURVED) tc::load8(tmem, (2 + tile) * tc::kCols, xiG);
+        if (t < T::LINES && (e % TX) < txe && (e / TX) < tye)
+        {
+            if constexpr (GEO == GEO_CURVED)
+            {
+                const double* mt = a.metrics + ((int64_t(j0 + e / TX + a.row_base) * Nx + (i0 + e % TX)) * NN + l) * 4 + 2;
+#pragma unroll
+                for (int m = 0; m < N; ++m)
+                {
+                    const double2 me = __ldg(reinterpret_cast<const double2*>(mt + m * N * 4));
+                    sC[(e * 4 + eq) * NN + m * N + l] = R_t(me.x) * dF[m] + R_t(me.y) * dG[m];
+                }
+            }
+            else
+            {
+#pragma unroll
+                for (int m = 0; m < N; ++m) sC[(e * 4 + eq) * NN + m * N + l] = R_t(a.eta_y) * dG[m];
+            }
+        }
+        __syncthreads();
+    }
 
     // ---- P3: element rows (e, eq, l), equation fastest across lanes
     for (int t = tid; t < TE * 4 * N; t += BT)
@@ -816,9 +975,12 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
         if (tx >= txe || ty >= tye) continue;
         const S* Fr = sF + (e * 4 + eq) * NN + l * N;
         S fv[N];
+        if constexpr (!TC)
+        {
 #pragma unroll
-        for (int m = 0; m < N; ++m) fv[m] = Fr[m];
-        center_line<S, N>(fv);
+            for (int m = 0; m < N; ++m) fv[m] = Fr[m];
+            center_line<S, N>(fv);
+        }
         const R_t dLl = opL<R_t>(ops, l), dRl = opR<R_t>(ops, l);
         const S dxl = sDel[((e * 4 + 0) * 4 + eq) * N + l];
         const S dxr = sDel[((e * 4 + 1) * 4 + eq) * N + l];
@@ -835,7 +997,7 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
                                  ? (int64_t(j0 + ty) * Nx + (i0 + tx)) * 5 + (jc - jcol + 5) % 5
                                  : (int64_t(j0 + ty) * Nx + (i0 + tx));
         S gr[N];
-        if constexpr (GEO == GEO_CURVED)
+        if constexpr (GEO == GEO_CURVED && !TC)
         {
             const S* Gr = sG + (e * 4 + eq) * NN + l * N;
 #pragma unroll
@@ -846,14 +1008,24 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
         for (int k = 0; k < N; ++k)
         {
             S dF = S(0.0);
+            if constexpr (TC)
+                dF = xiF[k];
+            else
+            {
 #pragma unroll
-            for (int m = 0; m < N; ++m) dF = dF + opD<R_t>(ops, k * N + m) * fv[m];
+                for (int m = 0; m < N; ++m) dF = dF + opD<R_t>(ops, k * N + m) * fv[m];
+            }
             S R;
             if constexpr (GEO == GEO_CURVED)
             {
                 S dG = S(0.0);
+                if constexpr (TC)
+                    dG = xiG[k];
+                else
+                {
 #pragma unroll
-                for (int m = 0; m < N; ++m) dG = dG + opD<R_t>(ops, k * N + m) * gr[m];
+                    for (int m = 0; m < N; ++m) dG = dG + opD<R_t>(ops, k * N + m) * gr[m];
+                }
                 const double2 mx = __ldg(reinterpret_cast<const double2*>(
                     a.metrics + ((int64_t(j0 + ty + a.row_base) * Nx + (i0 + tx)) * NN + l * N + k) * 4));
                 R = (R_t(mx.x) * dF + R_t(mx.y) * dG) + sC[(e * 4 + eq) * NN + l * N + k];
@@ -893,27 +1065,38 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
             }
         }
     }
+    if constexpr (TC)
+    {
+        // every tcgen05.ld of the CTA is complete: warp 0 frees the columns
+        tc::fence_before_sync();
+        __syncthreads();
+        if (tid < 32)
+        {
+            tc::fence_after_sync();
+            tc::tmem_free(tmem, T::TC_COLS);
+        }
+    }
     if constexpr (post)
     {
-        __syncthreads();
-        stage_epilogue<T, N, GAS>(a, ops, i0, j0, txe, tye, sO, smem_raw);
+        if constexpr (!TC) __syncthreads();
+        stage_epilogue<T, N, GAS>(a, ops, i0, j0, txe, tye, sO, base);
     }
 }
 
-template <class S, int N, int GAS, int RIEM, int GEO, bool POST>
-__global__ void __launch_bounds__((Tile2D<S, N, GEO>::BT)) __maxnreg__((Tile2D<S, N, GEO>::MAXREG))
+template <class S, int N, int GAS, int RIEM, int GEO, bool POST, bool TC>
+__global__ void __launch_bounds__((Tile2D<S, N, GEO, 0, TC>::BT)) __maxnreg__((Tile2D<S, N, GEO, 0, TC>::MAXREG))
 fr2d_kernel(const __grid_constant__ Fr2dArgs a)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    fr2d_tile<S, N, GAS, RIEM, GEO, 0, POST>(a, a.ops, blockIdx.x, blockIdx.y, smem_raw);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    fr2d_tile<S, N, GAS, RIEM, GEO, 0, POST, TC>(a, a.ops, blockIdx.x, blockIdx.y, smem_raw);
 }
 
-template <class S, int N, int GAS, int RIEM, int GEO, bool POST>
+template <class S, int N, int GAS, int RIEM, int GEO, bool POST, bool TC = false>
 cudaError_t launch_fr2d_kernel_v(const Fr2dArgs& a, cudaStream_t st)
 {
-    using T = Tile2D<S, N, GEO>;
-    auto kern = fr2d_kernel<S, N, GAS, RIEM, GEO, POST>;
-    constexpr size_t bytes = POST ? T::bytes_post : T::bytes;
+    using T = Tile2D<S, N, GEO, 0, TC>;
+    auto kern = fr2d_kernel<S, N, GAS, RIEM, GEO, POST, TC>;
+    constexpr size_t bytes = POST ? T::bytes_post : T::bytes_launch;
     // kernel attributes are per device: set them once on each device that launches
     static bool attr_done[64] = {};
     int dev = 0;
@@ -936,6 +1119,15 @@ cudaError_t launch_fr2d_kernel_v(const Fr2dArgs& a, cudaStream_t st)
 template <class S, int N, int GAS, int RIEM, int GEO>
 cudaError_t launch_fr2d_kernel(const Fr2dArgs& a, cudaStream_t st)
 {
+    if constexpr (sizeof(S) == 4 && (N == 5 || N == 6))
+    {
+        // the FP32 face tiles with their derivative contractions on the tensor cores
+        if (a.tc && a.mode != MODE_JAC)
+        {
+            if (a.mode == MODE_STAGE && a.post) return launch_fr2d_kernel_v<S, N, GAS, RIEM, GEO, true, true>(a, st);
+            return launch_fr2d_kernel_v<S, N, GAS, RIEM, GEO, false, true>(a, st);
+        }
+    }
     if constexpr (scalar_traits<S>::words == 1)
     {
         if (a.mode == MODE_STAGE && a.post) return launch_fr2d_kernel_v<S, N, GAS, RIEM, GEO, true>(a, st);
@@ -1007,7 +1199,7 @@ template <class S, int N, int GAS, int RIEM, int VAR>
 __global__ void __launch_bounds__((Tile2D<S, N, GEO_AFFINE, VAR>::BT)) __maxnreg__((Tile2D<S, N, GEO_AFFINE, VAR>::MAXREG))
 fr2d_batch_kernel(const __grid_constant__ Fr2dBatchArgs b)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(16) unsigned long long sa_raw[(sizeof(Fr2dArgs) + 7) / 8];
     Fr2dArgs& sa = *reinterpret_cast<Fr2dArgs*>(sa_raw);
     constexpr int HEAD = int(offsetof(Fr2dArgs, ops) / 8);  // the arguments before the operators

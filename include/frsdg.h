@@ -136,7 +136,12 @@ typedef struct frsdg_config {
      * called there; cell averages by GLL quadrature, floor eps = min(pp_eps, rho_bar,
      * p_bar).  Default 0 (off), pp_eps 1e-13. */
     int32_t pp_limit;
-    int32_t pad1_;
+    /* FP32 residual of the mixed form (frsdg_residual_f32, frsdg_rk_stage_mixed, the
+     * FRSDG_STAGE_MIXED stages) at p = 4 and 5 (no counterpart in the reference): 1 = its
+     * derivative contractions run on the tensor cores (tcgen05, operands split into
+     * TF32 high and low parts, FP32 accumulation), 0 = FP32 FMAs on the CUDA cores.
+     * Other orders, FP64 and complex residuals and batch launches ignore it. */
+    int32_t mixed_tc;
     double  pp_eps;
 } frsdg_config;
 
@@ -366,6 +371,15 @@ int frsdg_check_state(frsdg_handle* h, const double* U, void* stream);
  * applied elementwise to the device array x[0..n) into y, for validation against
  * IEEE division and sqrt.  No handle needed. */
 int frsdg_device_math(int32_t op, const double* x, double* y, int64_t n, void* stream);
+
+/* The split-precision tensor-core contraction of the FP32 residual on its own, for
+ * validation (no counterpart in the reference; it stands for the derivative sums of
+ * compute_volume_term, physics_impl_2D.hpp:320-354): out[l][k] = sum_m D[k][m]
+ * v[l][m] for `lines` lines of n (2..8) FP32 values, D an n x n FP64 matrix, all
+ * device arrays.  Values and D are split into TF32 high and low parts and multiplied
+ * by tcgen05 MMAs with FP32 accumulation.  Synchronises the stream; returns
+ * FRSDG_ERR_CUDA if the MMA completion wait gave up. */
+int frsdg_tc_lines(int32_t n, const float* v, const double* D, float* out, int64_t lines, void* stream);
 
 /* Largest solution (in doubles) frsdg_post_step_static accepts: 4,194,304 (32 MiB
  * of scratch held on every device that loads the library). */

@@ -111,3 +111,89 @@ def test_mixed_vortex_matches_fp64_accuracy(ne, cuda):
             errs[mixed] = float(l2_error(wl.cfg, U, ex, J)[0])
         assert s.status() == 0
     assert errs[True] <= 1.1 * errs[False], errs
+
+
+# ---- the FP32 residual with its derivative contractions on the tensor cores --------
+# (cfg.mixed_tc = 1, p = 4 and 5).  Meshes whose sizes leave partial tiles on both axes.
+TC_CASES = {
+    "cart_vdw_hllc_p4_walls": dict(p=4, n_elems=(9, 5), box=(1.3, 0.9), riemann="hllc", gas="vdw",
+                                   vdw=(0.05, 0.02),
+                                   bcs={A.LEFT: OUT, A.RIGHT: A.BC_WALL, A.TOP: A.BC_WALL, A.BOTTOM: OUT}),
+    "cart_vdw_rusanov_p5_periodic": dict(p=5, n_elems=(7, 5), riemann="rusanov", gas="vdw", vdw=(0.05, 0.02),
+                                         bcs={A.LEFT: PER, A.RIGHT: PER, A.TOP: PER, A.BOTTOM: PER}),
+    "sinewarp_hllc_p4_periodic": CASES["sinewarp_hllc_p4_periodic"],
+    "sinewarp_rusanov_p5_periodic": dict(p=5, n_elems=(5, 7), box=(10.0, 10.0), riemann="rusanov",
+                                         geometry=A.GEOM_SINE_WARP, geom_params=(0.1, 0, 0, 0),
+                                         bcs={A.LEFT: PER, A.RIGHT: PER, A.TOP: PER, A.BOTTOM: PER}),
+    "bump_hllc_p5_inflow_outlet": dict(CASES["bump_hllc_p3_inflow_outlet"], p=5, n_elems=(11, 3)),
+}
+
+
+def _tc_cfg(name, tc=1):
+    cfg = make_config(dim=2, **TC_CASES[name])
+    cfg.mixed_tc = tc
+    return cfg
+
+
+@pytest.mark.parametrize("name", sorted(TC_CASES))
+def test_residual_f32_tensor_cores_match_oracle(name, cuda):
+    """The tensor-core FP32 residual against the FP64 oracle (FP32 tolerance) and against
+    the CUDA-core FP32 residual (the same arithmetic but for the contraction order)."""
+    cfg = _tc_cfg(name)
+    U32 = random_state(cfg, 31, amp=0.3).astype(np.float32)
+    ref = Oracle(cfg, threads=4).residual(0.2, U32.astype(np.float64))
+    got = {}
+    for tc in (1, 0):
+        cfg.mixed_tc = tc
+        with FRSolver(cfg) as s:
+            Ud = torch.from_numpy(U32).to(cuda)
+            R = torch.full_like(Ud, float("nan"))
+            s.residual_kernel_f32(0.2, Ud, R)
+            got[tc] = R.cpu().numpy()
+            assert s.status() == 0
+    err = rel_err(got[1], ref)
+    assert err <= TOL_FP32, f"{name}: tensor-core FP32 residual rel err {err:.3e}"
+    assert rel_err(got[1], got[0]) <= TOL_FP32
+
+
+@pytest.mark.parametrize("name", ["cart_vdw_hllc_p4_walls", "sinewarp_rusanov_p5_periodic"])
+def test_fused_mixed_stage_with_tensor_cores(name, cuda):
+    """A mixed stage with the filter and the limiter in its epilogue: tensor-core and
+    CUDA-core contractions agree to the FP32 tolerance of the stage increment."""
+    cfg = _tc_cfg(name)
+    cfg.apply_filter, cfg.pp_limit, cfg.pp_eps = 1, 1, 1e-8
+    U = random_state(cfg, 7, amp=0.2)
+    gamma = 0.01
+    outs = {}
+    for tc in (1, 0):
+        cfg.mixed_tc = tc
+        with FRSolver(cfg) as s:
+            d = torch.from_numpy(U).to(cuda)
+            out = torch.empty_like(d)
+            s.rk_stage_fused(0.0, d, out, A.STAGE_MIXED | A.STAGE_POST_STEP, gamma, a=d, alpha=1.0)
+            outs[tc] = out.cpu().numpy()
+            rhs = torch.empty_like(d)
+            s.rhs_func(0.0, d, rhs)
+            scale = float(rhs.abs().max())
+            assert s.status() == 0
+    # the filter's rows have absolute sums near one; the limiter leaves these states alone
+    assert np.max(np.abs(outs[1] - outs[0])) <= 2.0 * TOL_FP32 * gamma * scale
+
+
+def test_mixed_vortex_with_tensor_cores_matches_fp64_accuracy(cuda):
+    """Curved isentropic vortex, p = 4, RK4 to t = 1 with the tensor-core FP32 residual:
+    L2 density error within 10 % of the FP64 run's."""
+    wl = vortex_curved(n_elems=16, p=4)
+    errs = {}
+    for mixed in (False, True):
+        wl.cfg.mixed_tc = 1
+        with FRSolver(wl.cfg) as s:
+            x, y = node_coords(wl.cfg, cuda)
+            ex = pack2d(*exact_vortex(1.0, x, y))
+            J = node_jacobian(wl.cfg, cuda)
+            U = wl.init(cuda)
+            dt = cfl_time_step(wl.cfg, U, 0.05)
+            Integrator(s, "rk4", mixed=mixed).run(U, dt, t_end=1.0)
+            errs[mixed] = float(l2_error(wl.cfg, U, ex, J)[0])
+            assert s.status() == 0
+    assert errs[True] <= 1.1 * errs[False], errs
