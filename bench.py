@@ -706,6 +706,7 @@ def run_ours(args, ws, rank, local):
                         "seconds": sms / 1e3, "pseudo_time_steps": sst.steps, "rejected": sst.rejected,
                         "newton_iterations": sst.newton_iterations, "gmres_iterations": sst.gmres_iterations,
                         "residual_drop": sst.residual_drop, "converged": sst.residual_drop <= 1e-10,
+                        "ms_per_gmres_iteration": sms / max(sst.gmres_iterations, 1),
                         "scheme": "SER pseudo time (dt0 0.05, growth <= 3, steps that grow the residual 1.5x "
                                   "rejected), GMRES(60) <= 200, aggregate coarse level 4x4 + block Gauss-Seidel"}
                 return implicit

@@ -97,6 +97,10 @@ SIGNATURES = {
     "frsdg_batch_destroy": (C.c_int, [_P]),
     "frsdg_device_math": (C.c_int, [C.c_int32, _P, _P, C.c_int64, _P]),
     "frsdg_tc_lines": (C.c_int, [C.c_int32, _P, _P, _P, C.c_int64, _P]),
+    "frsdg_gmres_work_doubles": (C.c_int64, [C.c_int64]),
+    "frsdg_gmres_arnoldi": (C.c_int, [_P, C.c_int64, C.c_int32, _P, C.c_int64, _P, C.c_int32, _P, _P, _P, _P, _P,
+                                      _P]),
+    "frsdg_gmres_solve": (C.c_int, [_P, C.c_int32, _P, C.c_int32, _P, _P]),
     "frsdg_petsc_vec_record_bytes": (C.c_int, [C.c_int64, C.c_int32, C.POINTER(C.c_int64)]),
     "frsdg_petsc_vec_pack": (C.c_int, [_P, C.c_int64, C.c_int32, _P, _P]),
     "frsdg_reference_element": (C.c_int, [C.c_int32, _D, _P, _P, _P, _P, _P]),

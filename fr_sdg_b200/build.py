@@ -39,7 +39,7 @@ def _units() -> list[tuple[Path, Path, list[str]]]:
     units = []
     for n in N_VALUES:
         units.append((CSRC / "instances.cu", BUILD / f"instances_n{n}.o", [f"-DFRSDG_N={n}"]))
-    for name in ("capi.cu", "stab.cu", "setup_ops.cpp", "noalloc.cu", "jacobi.cu", "petsc_io.cu", "pplimit.cu", "batch.cu", "tc.cu"):
+    for name in ("capi.cu", "stab.cu", "setup_ops.cpp", "noalloc.cu", "jacobi.cu", "petsc_io.cu", "pplimit.cu", "batch.cu", "tc.cu", "krylov.cu"):
         units.append((CSRC / name, BUILD / (Path(name).stem + ".o"), []))
     return units
 

@@ -16,10 +16,11 @@ module is the PETSc-free equivalent on the GPU:
               P^T J P on piecewise-constant aggregates of elements, probed with 20
               JVPs (aggregates coloured (I + 2J) mod 5, four variables), inverted
               densely; applied before the element-block sweep;
-  * GMRES(m)  right-preconditioned, classical Gram-Schmidt applied twice (the
-              Arnoldi basis lives on the device; the small Hessenberg least-squares
-              problem is solved on the host with Givens rotations, Saad, "Iterative
-              Methods for Sparse Linear Systems", 2nd ed., section 6.5).
+  * GMRES(m)  right-preconditioned; every Arnoldi step (classical Gram-Schmidt with
+              the DGKS second pass, the Hessenberg column and its Givens rotations,
+              Saad, "Iterative Methods for Sparse Linear Systems", 2nd ed., section
+              6.5) runs in libfrsdg's kernels (frsdg_gmres_arnoldi); the host reads one
+              residual norm per step, two steps late, and one per restart cycle.
 
 With a change of variables (cond_sys) the state is primitive and the transient
 variable is M(U) = prim->cons (TSSetTransientVariable, 575): U_t is replaced by
@@ -37,7 +38,7 @@ import torch
 
 from . import _abi as A
 from ._abi import FrsdgError
-from .solver import FRSolver
+from .solver import FRSolver, _stream
 
 
 @dataclass
@@ -46,17 +47,120 @@ class GmresStats:
     residual: float  # final preconditioned-system residual estimate, relative to ||b||
 
 
-def gmres(matvec, precond, b: torch.Tensor, restart: int = 30, rtol: float = 1e-3, max_iter: int = 200) -> tuple[
-        torch.Tensor, GmresStats]:
-    """Solve A x = b, right-preconditioned: A M^-1 y = b, x = M^-1 y."""
+class _DeviceArnoldi:
+    """The Arnoldi step and the back substitution of GMRES(m) in libfrsdg
+    (frsdg_gmres_arnoldi, frsdg_gmres_solve): Gram-Schmidt with the DGKS second pass,
+    the Hessenberg column and its Givens rotations stay on the device."""
+
+    def __init__(self, n: int, device):
+        self.lib = A.lib()
+        self.n = n
+        self.work = torch.empty(int(self.lib.frsdg_gmres_work_doubles(n)), dtype=torch.float64, device=device)
+
+    def arnoldi(self, V, j, w, H, cs, sn, g, inv):
+        A.check(self.lib.frsdg_gmres_arnoldi(V.data_ptr(), V.stride(0), j, w.data_ptr(), self.n, H.data_ptr(),
+                                             H.stride(0), cs.data_ptr(), sn.data_ptr(), g.data_ptr(), inv.data_ptr(),
+                                             self.work.data_ptr(), _stream()), "frsdg_gmres_arnoldi")
+
+    def solve(self, H, g, k, y):
+        A.check(self.lib.frsdg_gmres_solve(H.data_ptr(), H.stride(0), g.data_ptr(), k, y.data_ptr(), _stream()),
+                "frsdg_gmres_solve")
+
+
+class _HostArnoldi:
+    """The same step in torch operations on host tensors: the CPU form of the driver's
+    numerics, for tests of the restart and convergence logic without a GPU."""
+
+    def arnoldi(self, V, j, w, H, cs, sn, g, inv):
+        Vj = V[: j + 1]
+        w0 = float(w @ w)
+        h = Vj @ w
+        w -= Vj.T @ h
+        w1 = float(w @ w)
+        if w1 < 0.5 * w0:  # DGKS: a second pass
+            h2 = Vj @ w
+            w -= Vj.T @ h2
+            h = h + h2
+            w1 = float(w @ w)
+        hn = math.sqrt(max(w1, 0.0))
+        H[: j + 1, j] = h
+        H[j + 1, j] = hn
+        for i in range(j):
+            a, b_ = float(H[i, j]), float(H[i + 1, j])
+            H[i, j] = cs[i] * a + sn[i] * b_
+            H[i + 1, j] = -sn[i] * a + cs[i] * b_
+        a, b_ = float(H[j, j]), float(H[j + 1, j])
+        den = math.hypot(a, b_)
+        c, s_ = (1.0, 0.0) if den == 0.0 else (a / den, b_ / den)
+        cs[j], sn[j] = c, s_
+        H[j, j] = c * a + s_ * b_
+        H[j + 1, j] = 0.0
+        gj = float(g[j])
+        g[j + 1] = -s_ * gj
+        g[j] = c * gj
+        inv[0] = 1.0 / hn if hn > 0.0 else 0.0
+
+    def solve(self, H, g, k, y):
+        for i in range(k - 1, -1, -1):
+            d = float(H[i, i])
+            y[i] = (float(g[i]) - float(H[i, i + 1:k] @ y[i + 1:k])) / d if d != 0.0 else 0.0
+
+
+class _LaggedNorm:
+    """|g[idx]| read back `lag` Arnoldi steps late: each step queues a copy of its new
+    residual norm into pinned host memory and waits only for the copy of `lag` steps ago,
+    so the host stays at most `lag` steps ahead of the GPU and the GPU never waits for
+    the host.  lag = 0 reads at once (host tensors)."""
+
+    def __init__(self, g: torch.Tensor, lag: int):
+        self.g, self.lag = g, lag
+        if lag:
+            self.buf = torch.empty(lag + 1, dtype=g.dtype, pin_memory=True)
+            self.ev = [torch.cuda.Event() for _ in range(lag + 1)]
+        self.count = 0
+
+    def reset(self) -> None:
+        self.count = 0
+
+    def push(self, idx: int) -> float | None:
+        if not self.lag:
+            return abs(float(self.g[idx]))
+        slot = self.count % (self.lag + 1)
+        self.buf[slot: slot + 1].copy_(self.g[idx: idx + 1], non_blocking=True)
+        self.ev[slot].record()
+        self.count += 1
+        if self.count <= self.lag:
+            return None
+        old = (self.count - 1 - self.lag) % (self.lag + 1)
+        self.ev[old].synchronize()
+        return abs(float(self.buf[old]))
+
+
+def gmres(matvec, precond, b: torch.Tensor, restart: int = 30, rtol: float = 1e-3, max_iter: int = 200,
+          lag: int = 2) -> tuple[torch.Tensor, GmresStats]:
+    """Solve A x = b, right-preconditioned: A M^-1 y = b, x = M^-1 y (GMRES(restart),
+    Saad, algorithm 6.9).  On CUDA tensors every Arnoldi step runs in libfrsdg's kernels
+    and the host reads one residual norm per step, `lag` steps late (the solve may take
+    up to `lag` extra steps past the tolerance; each cycle's true estimate is read once
+    at its end).  At most 256 steps per cycle."""
+    if restart > 256:
+        raise ValueError("gmres: at most 256 Arnoldi steps per cycle")
     n = b.numel()
     x = torch.zeros_like(b)
     bnorm = float(torch.linalg.vector_norm(b))
     if bnorm == 0.0:
         return x, GmresStats(0, 0.0)
-    V = torch.empty((restart + 1, n), dtype=b.dtype, device=b.device)
-    Z = torch.empty((restart, n), dtype=b.dtype, device=b.device)
+    dev = b.device
+    f64 = dict(dtype=torch.float64, device=dev)
+    V = torch.empty((restart + 1, n), dtype=b.dtype, device=dev)
+    Z = torch.empty((restart, n), dtype=b.dtype, device=dev)
     w = torch.empty_like(b)
+    H = torch.zeros((restart + 1, restart), **f64)
+    cs, sn, y = torch.zeros(restart, **f64), torch.zeros(restart, **f64), torch.zeros(restart, **f64)
+    g = torch.zeros(restart + 1, **f64)
+    inv = torch.zeros(1, **f64)
+    step = _DeviceArnoldi(n, dev) if b.is_cuda else _HostArnoldi()
+    probe = _LaggedNorm(g, lag if b.is_cuda else 0)
     total = 0
     rel = 1.0
     r = b.clone()
@@ -65,46 +169,25 @@ def gmres(matvec, precond, b: torch.Tensor, restart: int = 30, rtol: float = 1e-
         rel = beta / bnorm
         if rel <= rtol:
             break
-        V[0] = r / beta
-        H = np.zeros((restart + 1, restart))
-        cs = np.zeros(restart)
-        sn = np.zeros(restart)
-        g = np.zeros(restart + 1)
+        torch.div(r, beta, out=V[0])
+        H.zero_()
+        g.zero_()
         g[0] = beta
+        probe.reset()
         k = 0
         for j in range(restart):
             precond(V[j], Z[j])
             matvec(Z[j], w)
-            h = V[: j + 1] @ w
-            w -= V[: j + 1].T @ h
-            h2 = V[: j + 1] @ w
-            w -= V[: j + 1].T @ h2
-            # the new Hessenberg column and ||w|| in one device-to-host read
-            hn_dev = torch.linalg.vector_norm(w).reshape(1)
-            col = torch.cat((h + h2, hn_dev)).cpu().numpy()
-            h, hn = col[:-1], float(col[-1])
-            H[: j + 1, j] = h
-            H[j + 1, j] = hn
-            for i in range(j):
-                t0 = cs[i] * H[i, j] + sn[i] * H[i + 1, j]
-                H[i + 1, j] = -sn[i] * H[i, j] + cs[i] * H[i + 1, j]
-                H[i, j] = t0
-            den = math.hypot(H[j, j], H[j + 1, j])
-            cs[j], sn[j] = (1.0, 0.0) if den == 0.0 else (H[j, j] / den, H[j + 1, j] / den)
-            H[j, j] = cs[j] * H[j, j] + sn[j] * H[j + 1, j]
-            H[j + 1, j] = 0.0
-            g[j + 1] = -sn[j] * g[j]
-            g[j] = cs[j] * g[j]
+            step.arnoldi(V, j, w, H, cs, sn, g, inv)
+            torch.mul(w, inv, out=V[j + 1])
             k = j + 1
             total += 1
-            rel = abs(g[j + 1]) / bnorm
-            if rel <= rtol or hn == 0.0 or total >= max_iter:
+            seen = probe.push(j + 1)
+            if (seen is not None and seen <= rtol * bnorm) or total >= max_iter:
                 break
-            torch.div(w, hn_dev, out=V[j + 1])
-        y = np.zeros(k)
-        for i in range(k - 1, -1, -1):
-            y[i] = (g[i] - H[i, i + 1:k] @ y[i + 1:k]) / H[i, i]
-        x += Z[:k].T @ torch.from_numpy(y).to(b.device)
+        step.solve(H, g, k, y)
+        x.addmv_(Z[:k].T, y[:k])
+        rel = abs(float(g[k])) / bnorm
         if rel <= rtol or total >= max_iter:
             break
         matvec(x, w)

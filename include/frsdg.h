@@ -270,6 +270,27 @@ int frsdg_jac_blocks5(frsdg_handle* h, double t, double sigma, const double* U,
 int frsdg_pc_setup_gs(frsdg_handle* h, double t, double sigma, const double* U, void* stream);
 int frsdg_pc_apply(frsdg_handle* h, const double* r, double* z, void* stream);
 
+/* Restarted GMRES on the device: the Krylov solver PETSc's KSPGMRES runs for every
+ * Newton system of the implicit path (petsc_solver_impl.hpp:549-612; the reference
+ * leaves it to PETSc), without a host round trip per iteration.  All arrays are device
+ * memory; nothing is allocated.
+ * frsdg_gmres_work_doubles: size (in doubles) of the scratch array `work` for vectors
+ *   of n entries.
+ * frsdg_gmres_arnoldi: Arnoldi step j (0 <= j < 256) on the basis V[0..j] (row i of V at
+ *   V + i*ldv, n entries each): w <- w - V h by classical Gram-Schmidt, repeated once
+ *   when the first pass leaves ||w||^2 below half its value; column j of the row-major
+ *   Hessenberg H (leading dimension ldh > j, j + 2 rows) gets h and ||w||, then the
+ *   previous Givens rotations (cs, sn) and a new one that zeroes H[j+1][j]; the
+ *   least-squares residual vector g turns with it (|g[j+1]| is the new residual norm);
+ *   *inv_hn = 1/||w|| (0 when w vanished), the scale of the next basis vector.
+ * frsdg_gmres_solve: y = R^-1 g on the first k columns of the rotated H (back
+ *   substitution; a zero diagonal leaves y at 0 there).
+ * Reductions run in a fixed order: repeated calls give identical results. */
+int64_t frsdg_gmres_work_doubles(int64_t n);
+int frsdg_gmres_arnoldi(const double* V, int64_t ldv, int32_t j, double* w, int64_t n, double* H, int32_t ldh,
+                        double* cs, double* sn, double* g, double* inv_hn, double* work, void* stream);
+int frsdg_gmres_solve(const double* H, int32_t ldh, const double* g, int32_t k, double* y, void* stream);
+
 /* One explicit Runge-Kutta stage fused into the residual pass:
  *   out = alpha*A + beta*B + gamma*rhs(Us),   acc += delta*rhs(Us)   (rhs = -R)
  * A, B and acc may be NULL (the term is dropped).  out must not alias Us (the

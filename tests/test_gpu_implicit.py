@@ -327,3 +327,76 @@ def test_full_bump_reaches_steady_state(cuda):
                              max_growth=3.0, reject_growth=1.5)
         assert s.status() == 0
     assert st.residual_drop <= 1e-10, st.history[-6:]
+
+
+# ---- GMRES with the Arnoldi step on the device (frsdg_gmres_arnoldi) -------------------
+def _dense_system(n, seed):
+    g = torch.Generator().manual_seed(seed)
+    Am = torch.eye(n, dtype=torch.float64) + 0.3 * torch.randn(n, n, generator=g, dtype=torch.float64) / n ** 0.5
+    b = torch.randn(n, generator=g, dtype=torch.float64)
+    return Am, b
+
+
+@pytest.mark.parametrize("restart", [7, 30])
+def test_device_gmres_matches_host_arnoldi(restart, cuda):
+    """The device Arnoldi step against its host restatement on the same system: the
+    same solution, and the device run takes at most two extra steps (its convergence
+    check reads the residual norm two steps late)."""
+    from fr_sdg_b200.implicit import gmres
+
+    Am, b = _dense_system(2000, 5)
+    xh, sh = gmres(lambda v, o: o.copy_(Am @ v), lambda r, z: z.copy_(r), b, restart=restart, rtol=1e-9,
+                   max_iter=400)
+    Ad, bd = Am.to(cuda), b.to(cuda)
+    xd, sd = gmres(lambda v, o: torch.mv(Ad, v, out=o), lambda r, z: z.copy_(r), bd, restart=restart, rtol=1e-9,
+                   max_iter=400)
+    assert 0 <= sd.iterations - sh.iterations <= 2
+    assert sd.residual <= 1e-9
+    true_rel = float(torch.linalg.vector_norm(bd - Ad @ xd) / torch.linalg.vector_norm(bd))
+    assert true_rel <= 2e-9
+    assert float(torch.linalg.vector_norm(xd.cpu() - xh) / torch.linalg.vector_norm(xh)) <= 1e-8
+
+
+def test_device_gmres_breakdown_and_repeatability(cuda):
+    """A = 2 I: the Krylov space closes after one step (||w|| = 0); the solution is exact
+    and the extra steps after the breakdown leave it alone.  Two solves of the same
+    system give identical bits (fixed-order reductions)."""
+    from fr_sdg_b200.implicit import gmres
+
+    b = torch.randn(10_000, dtype=torch.float64, device=cuda)
+    x, st = gmres(lambda v, o: torch.mul(v, 2.0, out=o), lambda r, z: z.copy_(r), b, restart=10, rtol=1e-12)
+    assert torch.allclose(x, 0.5 * b, rtol=0, atol=1e-14)
+    assert st.residual <= 1e-12
+    Am, bb = _dense_system(3000, 9)
+    Ad, bd = Am.to(cuda), bb.to(cuda)
+    run = lambda: gmres(lambda v, o: torch.mv(Ad, v, out=o), lambda r, z: z.copy_(r), bd, restart=20, rtol=1e-10,
+                        max_iter=300)[0]
+    assert torch.equal(run(), run())
+
+
+def test_arnoldi_step_orthogonality(cuda):
+    """After m device Arnoldi steps on D = diag(1 + U(0, 1)) the basis is orthonormal to
+    rounding: D v_j lies mostly along v_j (||w|| drops below 1/sqrt(2) of its value in the
+    first Gram-Schmidt pass), so every step takes the second pass."""
+    from fr_sdg_b200.implicit import _DeviceArnoldi
+
+    n, m = 50_000, 12
+    g = torch.Generator(device=cuda).manual_seed(3)
+    d = 1.0 + torch.rand(n, generator=g, dtype=torch.float64, device=cuda)
+    V = torch.zeros((m + 1, n), dtype=torch.float64, device=cuda)
+    V[0] = torch.randn(n, generator=g, dtype=torch.float64, device=cuda)
+    V[0] /= torch.linalg.vector_norm(V[0])
+    H = torch.zeros((m + 1, m), dtype=torch.float64, device=cuda)
+    cs, sn = torch.zeros(m, dtype=torch.float64, device=cuda), torch.zeros(m, dtype=torch.float64, device=cuda)
+    gg = torch.zeros(m + 1, dtype=torch.float64, device=cuda)
+    gg[0] = 1.0
+    inv = torch.zeros(1, dtype=torch.float64, device=cuda)
+    w = torch.empty(n, dtype=torch.float64, device=cuda)
+    step = _DeviceArnoldi(n, cuda)
+    for j in range(m):
+        torch.mul(d, V[j], out=w)
+        step.arnoldi(V, j, w, H, cs, sn, gg, inv)
+        torch.mul(w, inv, out=V[j + 1])
+    Q = V[:m]
+    err = float((Q @ Q.T - torch.eye(m, dtype=torch.float64, device=cuda)).abs().max())
+    assert err <= 1e-12
