@@ -412,7 +412,7 @@ def run_ours(args, ws, rank, local):
     # mixed form (FP32 arithmetic on the FP64 state, node primitives recovered in FP64),
     # device-resident
     mixed = None
-    if not args.no_t_end and ws == 1:
+    if not args.no_mixed and ws == 1:
         U32 = U.float()
         F32 = torch.empty_like(U32)
         out = torch.empty_like(U)
@@ -767,6 +767,7 @@ def main(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-t-end", action="store_true", help="skip the 200-step time-to-t_end run")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the FP32 / mixed-precision residual figures")
     ap.add_argument("--cpu-all-cores", action="store_true")
     args = ap.parse_args(argv)
     if args.warmup < 3 and args.impl == "ours":

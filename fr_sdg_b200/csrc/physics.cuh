@@ -20,13 +20,19 @@ template <class S> __device__ __forceinline__ S cs(double v) { return S(v); }
 template <> __device__ __forceinline__ float cs<float>(double v) { return static_cast<float>(v); }
 
 // macro_and_libc.hpp:80-113
-template <class S> __device__ __forceinline__ S smooth_abs(S v)
+template <class S, class M = MathChecked> __device__ __forceinline__ S smooth_abs(S v, const M& m = M{})
 {
     const S eps = cs<S>(1e-7);
-    return s_sqrt(v * v + eps * eps) - eps;
+    return m.sqrt(v * v + eps * eps) - eps;
 }
-template <class S> __device__ __forceinline__ S smooth_max(S a, S b) { return cs<S>(0.5) * (a + b + smooth_abs(a - b)); }
-template <class S> __device__ __forceinline__ S smooth_min(S a, S b) { return cs<S>(0.5) * (a + b - smooth_abs(a - b)); }
+template <class S, class M = MathChecked> __device__ __forceinline__ S smooth_max(S a, S b, const M& m = M{})
+{
+    return cs<S>(0.5) * (a + b + smooth_abs(a - b, m));
+}
+template <class S, class M = MathChecked> __device__ __forceinline__ S smooth_min(S a, S b, const M& m = M{})
+{
+    return cs<S>(0.5) * (a + b - smooth_abs(a - b, m));
+}
 
 // gas_models.hpp:56-87 (GAS == 0) and 89-158 (GAS == 1)
 template <int GAS, class S> __device__ __forceinline__ S gas_pressure(const GasParams& g, S rho, S e)
@@ -168,44 +174,63 @@ template <class S> struct NodePrim
     S rho_w, inv_rho, u, v, e, p, inv_covol;
 };
 
-template <int GAS, class S>
-__device__ __forceinline__ NodePrim<S> node_prim(const GasParams& g, S r0, S r1, S r2, S r3)
+// Products and multiply-adds with a fixed rounding: the compiler neither fuses pmul
+// with a neighbouring addition nor splits pfma, so every inlined copy of the node
+// primitives rounds alike (tile nodes and the halo nodes of a neighbouring tile give the
+// same bits).  Complex: the textbook product with one explicit multiply-add per part.
+__device__ __forceinline__ double pmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float pmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ cplx pmul(cplx a, cplx b)
+{
+    return {fma(a.re, b.re, -__dmul_rn(a.im, b.im)), fma(a.re, b.im, __dmul_rn(a.im, b.re))};
+}
+__device__ __forceinline__ double pfma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float pfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ cplx pfma(cplx a, cplx b, cplx c) { return pmul(a, b) + c; }
+
+template <int GAS, class S, class M = MathChecked>
+__device__ __forceinline__ NodePrim<S> node_prim(const GasParams& g, S r0, S r1, S r2, S r3, const M& m = M{})
 {
     NodePrim<S> q;
     q.rho_w   = s_wrap_positive(r0);
-    q.inv_rho = s_rcp(q.rho_w);
-    q.u       = r1 * q.inv_rho;
-    q.v       = r2 * q.inv_rho;
+    q.inv_rho = m.rcp(q.rho_w);
+    q.u       = pmul(r1, q.inv_rho);
+    q.v       = pmul(r2, q.inv_rho);
     const S E = s_wrap_positive(r3);
-    q.e       = E * q.inv_rho - cs<S>(0.5) * (q.u * q.u + q.v * q.v);
+    // e = E / rho - (u^2 + v^2) / 2
+    q.e       = pfma(E, q.inv_rho, pmul(cs<S>(-0.5), pfma(q.u, q.u, pmul(q.v, q.v))));
+    const S gm1 = cs<S>(g.gamma) - cs<S>(1.0);
     if constexpr (GAS == FRSDG_GAS_IDEAL)
     {
         q.inv_covol = cs<S>(1.0);
-        q.p         = (cs<S>(g.gamma) - cs<S>(1.0)) * q.rho_w * q.e;
+        q.p         = pmul(pmul(gm1, q.rho_w), q.e);
     }
     else
     {
-        q.inv_covol = s_rcp(cs<S>(1.0) - cs<S>(g.b) * q.rho_w);
-        const S cvT = q.e + cs<S>(g.a) * q.rho_w;
-        q.p = ((cs<S>(g.gamma) - cs<S>(1.0)) * q.rho_w * cvT) * q.inv_covol - cs<S>(g.a) * q.rho_w * q.rho_w;
+        // p = (gamma - 1) rho (e + a rho) / (1 - b rho) - a rho^2
+        q.inv_covol = m.rcp(pfma(cs<S>(-g.b), q.rho_w, cs<S>(1.0)));
+        const S cvT = pfma(cs<S>(g.a), q.rho_w, q.e);
+        q.p = pfma(pmul(pmul(gm1, q.rho_w), cvT), q.inv_covol, -pmul(pmul(cs<S>(g.a), q.rho_w), q.rho_w));
     }
     return q;
 }
 
-template <int GAS, class S>
-__device__ __forceinline__ S node_sound_speed(const GasParams& g, const NodePrim<S>& q)
+template <int GAS, class S, class M = MathChecked>
+__device__ __forceinline__ S node_sound_speed(const GasParams& g, const NodePrim<S>& q, const M& m = M{})
 {
     if constexpr (GAS == FRSDG_GAS_IDEAL)
-        return s_sqrt(cs<S>(g.gamma) * q.p * q.inv_rho);
+        return m.sqrt(pmul(pmul(cs<S>(g.gamma), q.p), q.inv_rho));
     else
     {
-        const S inv_dsq = q.inv_covol * q.inv_covol;
-        const S thermal = q.e + cs<S>(g.a) * q.rho_w;
+        // c^2 = gamma (gamma - 1) (e + a rho) / (1 - b rho)^2
+        //       + (gamma - 1) a rho (2 - b rho) / (1 - b rho)^2 - 2 a rho
+        const S inv_dsq = pmul(q.inv_covol, q.inv_covol);
+        const S thermal = pfma(cs<S>(g.a), q.rho_w, q.e);
         const S gm1     = cs<S>(g.gamma) - cs<S>(1.0);
-        const S term1   = (cs<S>(g.gamma) * gm1 * thermal) * inv_dsq;
-        const S term2   = (gm1 * cs<S>(g.a) * q.rho_w * (cs<S>(2.0) - cs<S>(g.b) * q.rho_w)) * inv_dsq;
-        const S term3   = cs<S>(2.0) * cs<S>(g.a) * q.rho_w;
-        return s_sqrt(term1 + term2 - term3);
+        const S term1   = pmul(pmul(pmul(cs<S>(g.gamma), gm1), thermal), inv_dsq);
+        const S term2   = pmul(pmul(pmul(pmul(gm1, cs<S>(g.a)), q.rho_w), pfma(cs<S>(-g.b), q.rho_w, cs<S>(2.0))), inv_dsq);
+        const S term3   = pmul(pmul(cs<S>(2.0), cs<S>(g.a)), q.rho_w);
+        return m.sqrt(term1 + term2 - term3);
     }
 }
 
@@ -217,8 +242,9 @@ enum RecField : int
 };
 
 // RiemannSolver2D (riemann_solver.hpp:189-349) on two face records.
-template <int RIEM, class S>
-__device__ __forceinline__ void riemann_rec(const S L[RF_N], const S R[RF_N], double nx_, double ny_, S Fs[4])
+template <int RIEM, class S, class M = MathChecked>
+__device__ __forceinline__ void riemann_rec(const S L[RF_N], const S R[RF_N], double nx_, double ny_, S Fs[4],
+                                            const M& m = M{})
 {
     using real    = typename scalar_traits<S>::real;
     const real nx = static_cast<real>(nx_), ny = static_cast<real>(ny_);
@@ -234,7 +260,7 @@ __device__ __forceinline__ void riemann_rec(const S L[RF_N], const S R[RF_N], do
     S f0, f1, f2, f3;
     if constexpr (RIEM == FRSDG_RUSANOV)
     {
-        const S smax = smooth_max(smooth_abs(unL) + cL, smooth_abs(unR) + cR);
+        const S smax = smooth_max(smooth_abs(unL, m) + cL, smooth_abs(unR, m) + cR, m);
         const S h    = cs<S>(0.5);
         f0 = h * (FL0 + FR0) - h * smax * (R[RF_RHO] - L[RF_RHO]);
         f1 = h * (FL1 + FR1) - h * smax * (R[RF_RHO] * unR - L[RF_RHO] * unL);
@@ -243,11 +269,11 @@ __device__ __forceinline__ void riemann_rec(const S L[RF_N], const S R[RF_N], do
     }
     else
     {
-        const S sL = smooth_min(unL - cL, unR - cR);
-        const S sR = smooth_max(unL + cL, unR + cR);
+        const S sL = smooth_min(unL - cL, unR - cR, m);
+        const S sR = smooth_max(unL + cL, unR + cR, m);
         const S rhoL_diff = L[RF_RHO] * (sL - unL);
         const S rhoR_diff = R[RF_RHO] * (sR - unR);
-        const S sM = (pR - pL + unL * rhoL_diff - unR * rhoR_diff) * s_rcp(rhoL_diff - rhoR_diff);
+        const S sM = (pR - pL + unL * rhoL_diff - unR * rhoR_diff) * m.rcp(rhoL_diff - rhoR_diff);
         const bool left = s_branch(sM) >= 0.0;
         const S K0 = left ? L[RF_RHO] : R[RF_RHO];
         const S K3 = left ? L[RF_E] : R[RF_E];
@@ -257,7 +283,7 @@ __device__ __forceinline__ void riemann_rec(const S L[RF_N], const S R[RF_N], do
         const S pK = left ? pL : pR;
         const S FK0 = left ? FL0 : FR0, FK1 = left ? FL1 : FR1, FK3 = left ? FL3 : FR3;
         const S p_star = pK + K0 * (sK - unK) * (sM - unK);
-        const S inv = s_rcp(sK - sM);
+        const S inv = m.rcp(sK - sM);
         const S st0 = (sM * (sK * K0 - FK0)) * inv;
         const S st1 = (sM * (sK * (K0 * unK) - FK1) + sK * p_star) * inv;
         const S st2 = utK * st0;

@@ -18,6 +18,7 @@
 // compile-time indices; tile loops have compile-time trip counts.
 #pragma once
 #include <cstddef>
+#include <type_traits>
 
 #include "device_math.cuh"
 #include "frsdg_internal.hpp"
@@ -693,24 +694,33 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
             hrec = r;
         }
     }
-    for (int q = tid; q < TE * NN; q += BT)
-    {
+    // One tile node: load, primitives, fluxes to sF / sG and (boundary nodes) the face
+    // record.  Run with MathDeferred, `bad` tells whether a reciprocal or square root met
+    // an input outside the fast range; such nodes are redone after the loop with
+    // MathChecked, so that the loop itself stays free of those branches.  (A halo record
+    // must equal, bit for bit, the record of the same node computed inside a tile, since
+    // row windows move tile edges: node_prim and node_sound_speed pin their operations
+    // with explicit multiply-adds, so that every inlined copy rounds alike.)
+    auto node_pass = [&](int q, const auto& m) {
         const int e = q / NN, node = q % NN, tx = e % TX, ty = e / TX, k = node % N, l = node / N;
         if (tx < txe && ty < tye)
         {
             const int64_t off = (int64_t(j0 + ty) * Nx + (i0 + tx)) * ND + node * 4;
             const bool bnode = k == 0 || k == N - 1 || l == 0 || l == N - 1;
-            S s[4], c64 = S(0.0);
+            S s[4], c = S(0.0);
             NodePrim<S> pr;
-            const bool f64 = node_state_f64<GAS>(a, g, off, s, pr, bnode ? &c64 : nullptr);
+            const bool f64 = node_state_f64<GAS>(a, g, off, s, pr, bnode ? &c : nullptr);
             if (!f64) NodeLoader<S>::load(a, off, s);
             if constexpr (T::JVP)
             {
 #pragma unroll
                 for (int eq = 0; eq < 4; ++eq) sSeed[(e * 4 + eq) * NN + node] = s_im(s[eq]);
             }
-            if (!density_ok(s_re(s[0])) && a.bad) atomicAdd(a.bad, 1ull);
-            if (!f64) pr = node_prim<GAS>(g, s[0], s[1], s[2], s[3]);
+            if (!f64)
+            {
+                pr = node_prim<GAS>(g, s[0], s[1], s[2], s[3], m);
+                if (bnode) c = node_sound_speed<GAS>(g, pr, m);
+            }
             const S rEp = s[3] + pr.p;
             const S ruv = s[1] * pr.v;
             S* f = sF + e * 4 * NN + node;
@@ -725,26 +735,52 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
             gg[3 * NN] = pr.v * rEp;
             if (bnode)
             {
-                S rec[RF_N];
-                make_record<GAS>(g, s, pr, rec);
-                if (f64) rec[RF_C] = c64;
+                const S rec[RF_N] = {s[0], s[3], pr.u, pr.v, pr.p, c};
                 const int r = e * T::NB + T::bidx(k, l);
 #pragma unroll
                 for (int fld = 0; fld < RF_N; ++fld) sRec[fld * NREC + r] = rec[fld];
             }
+            return s_re(s[0]);
         }
-    }
-    if (hrec >= 0)
-    {
+        return 1.0;
+    };
+    auto halo_pass = [&](const auto& m) {
         NodePrim<S> pr;
-        S c64 = S(0.0);
-        const bool f64 = node_state_f64<GAS>(a, g, hoff, hs, pr, &c64);
-        if (!f64) pr = node_prim<GAS>(g, hs[0], hs[1], hs[2], hs[3]);
-        S rec[RF_N];
-        make_record<GAS>(g, hs, pr, rec);
-        if (f64) rec[RF_C] = c64;
+        S c = S(0.0);
+        const bool f64 = node_state_f64<GAS>(a, g, hoff, hs, pr, &c);
+        if (!f64)
+        {
+            pr = node_prim<GAS>(g, hs[0], hs[1], hs[2], hs[3], m);
+            c = node_sound_speed<GAS>(g, pr, m);
+        }
+        const S rec[RF_N] = {hs[0], hs[3], pr.u, pr.v, pr.p, c};
 #pragma unroll
         for (int fld = 0; fld < RF_N; ++fld) sRec[fld * NREC + hrec] = rec[fld];
+    };
+    static_assert((TE * NN + BT - 1) / BT < 31, "node iterations fit the redo mask");
+    unsigned redo = 0;  // bit i: this thread's node i (bit 31: its halo node) to redo
+    {
+        int it = 0;
+        for (int q = tid; q < TE * NN; q += BT, ++it)
+        {
+            unsigned bad = 0;
+            const double rho = node_pass(q, MathDeferred{bad});
+            if (!density_ok(rho) && a.bad) atomicAdd(a.bad, 1ull);
+            redo |= bad << it;
+        }
+        if (hrec >= 0)
+        {
+            unsigned bad = 0;
+            halo_pass(MathDeferred{bad});
+            redo |= bad << 31;
+        }
+    }
+    if (redo)
+    {
+        int it = 0;
+        for (int q = tid; q < TE * NN; q += BT, ++it)
+            if ((redo >> it) & 1u) node_pass(q, MathChecked{});
+        if (redo >> 31) halo_pass(MathChecked{});
     }
     if constexpr (TC)
     {
@@ -861,28 +897,39 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
             }
         }
     };
+    // One face point (x-faces: XF): both side records, the boundary ghost, the Riemann
+    // flux and the jumps; with MathDeferred, `bad` tells whether to redo it with
+    // MathChecked (after the hot code, like the node pass).
+    auto face_point = [&](auto xf_tag, int t, bool exists, const auto& m) {
+        constexpr bool XF = decltype(xf_tag)::value;
+        FaceSide<S> sd[2];
+        S Fs[4];
+        if (face_prepare<S, N, GEO, XF, T>(a, exists, t, i0, j0, txe, tye, sRec, sd))
+        {
+            if (sd[0].bc || sd[1].bc) face_ghost<GAS, S, N, XF, T>(a, i0, j0, sd);
+            riemann_rec<RIEM>(sd[0].R, sd[1].R, sd[0].nx, sd[0].ny, Fs, m);
+            face_jumps<S, N, GEO, XF, T>(a, i0, j0, true, sd, Fs, sF, sG, sDel);
+        }
+    };
+    using XFace = std::true_type;
+    using YFace = std::false_type;
     if constexpr (UNPAIR)
     {
         if (tid < PX + PY)
         {
             const bool xf = tid < PX;
             const int t = xf ? tid : tid - PX;
-            FaceSide<S> sd[2];
-            S Fs[4];
+            unsigned bad = 0;
             if (xf)
+                face_point(XFace{}, t, t < NXF, MathDeferred{bad});
+            else
+                face_point(YFace{}, t, t < NYF, MathDeferred{bad});
+            if (bad)
             {
-                if (face_prepare<S, N, GEO, true, T>(a, t < NXF, t, i0, j0, txe, tye, sRec, sd))
-                {
-                    if (sd[0].bc || sd[1].bc) face_ghost<GAS, S, N, true, T>(a, i0, j0, sd);
-                    riemann_rec<RIEM>(sd[0].R, sd[1].R, sd[0].nx, sd[0].ny, Fs);
-                    face_jumps<S, N, GEO, true, T>(a, i0, j0, true, sd, Fs, sF, sG, sDel);
-                }
-            }
-            else if (face_prepare<S, N, GEO, false, T>(a, t < NYF, t, i0, j0, txe, tye, sRec, sd))
-            {
-                if (sd[0].bc || sd[1].bc) face_ghost<GAS, S, N, false, T>(a, i0, j0, sd);
-                riemann_rec<RIEM>(sd[0].R, sd[1].R, sd[0].nx, sd[0].ny, Fs);
-                face_jumps<S, N, GEO, false, T>(a, i0, j0, true, sd, Fs, sF, sG, sDel);
+                if (xf)
+                    face_point(XFace{}, t, t < NXF, MathChecked{});
+                else
+                    face_point(YFace{}, t, t < NYF, MathChecked{});
             }
         }
         else if constexpr (!TC)
@@ -918,10 +965,16 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
                 if (xs[0].bc || xs[1].bc) face_ghost<GAS, S, N, true, T>(a, i0, j0, xs);
                 if (ys[0].bc || ys[1].bc) face_ghost<GAS, S, N, false, T>(a, i0, j0, ys);
                 S Fx[4], Fy[4];
-                riemann_rec<RIEM>(xs[0].R, xs[1].R, xs[0].nx, xs[0].ny, Fx);
-                riemann_rec<RIEM>(ys[0].R, ys[1].R, ys[0].nx, ys[0].ny, Fy);
+                unsigned bad = 0;
+                riemann_rec<RIEM>(xs[0].R, xs[1].R, xs[0].nx, xs[0].ny, Fx, MathDeferred{bad});
+                riemann_rec<RIEM>(ys[0].R, ys[1].R, ys[0].nx, ys[0].ny, Fy, MathDeferred{bad});
                 face_jumps<S, N, GEO, true, T>(a, i0, j0, vx, xs, Fx, sF, sG, sDel);
                 face_jumps<S, N, GEO, false, T>(a, i0, j0, vy, ys, Fy, sF, sG, sDel);
+                if (bad)
+                {
+                    if (vx) face_point(XFace{}, t, t < NXF, MathChecked{});
+                    if (vy) face_point(YFace{}, t, t < NYF, MathChecked{});
+                }
             }
             else if (t - PFP < NCOL)
                 column(t - PFP);

@@ -187,3 +187,25 @@ def test_post_step_to_equals_in_place(stab, cuda):
         assert torch.equal(dst, ref)
         assert torch.equal(src, U)
         assert A.lib().frsdg_post_step_to(s._h, src.data_ptr(), src.data_ptr(), None) == A.ERR_ARG
+
+
+@pytest.mark.parametrize("scale", [1e-150, 1e150])
+@pytest.mark.parametrize("name", ["cart_ideal_hllc_p7", "cart_ideal_rusanov_p3", "sinewarp_hllc_p4_periodic"])
+def test_residual_outside_float_range(name, scale, cuda):
+    """Every conservative value scaled by 1e-150 or 1e150: densities, pressures and the
+    HLLC denominators leave the range where the FP64 reciprocal and square root take
+    their single-precision seeds, so every node and face point is redone with the
+    checked IEEE operations; the residual (R scales with the state for an ideal gas)
+    still equals the oracle's."""
+    cfg = _cfg2d(**CASES_2D[name])
+    U = random_state(cfg, seed=77) * scale
+    ref = Oracle(cfg, threads=4).residual(0.2, U)
+    assert np.all(np.isfinite(ref))
+    with FRSolver(cfg) as s:
+        Ud = _dev(U, cuda)
+        R = torch.empty_like(Ud)
+        s.residual_kernel(0.2, Ud, R)
+        got = R.cpu().numpy()
+        assert s.status() == 0
+    err = rel_err(got, ref)
+    assert err <= TOL_FP64, f"{name} x {scale:g}: rel err {err:.3e}"
