@@ -160,8 +160,25 @@ struct MathDeferred
         bad |= positive_in_float_range(x) ? 0u : 1u;
         return sqrt_fast(x);
     }
-    __device__ __forceinline__ float rcp(float x) const { return s_rcp(x); }
-    __device__ __forceinline__ float sqrt(float x) const { return s_sqrt(x); }
+    // FP32: the hardware approximations with one Newton step (within 2 ulp of the IEEE
+    // results) for normal inputs whose results stay normal; zero, subnormals, huge values,
+    // inf and NaN (exponent tests as above) take the redo with the IEEE operations
+    __device__ __forceinline__ float rcp(float x) const
+    {
+        const unsigned e = (__float_as_uint(x) >> 23) & 0xffu;
+        bad |= e - 2u < 250u ? 0u : 1u;  // 2^-125 <= |x| < 2^125
+        float r;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+        return fmaf(r, fmaf(-x, r, 1.0f), r);
+    }
+    __device__ __forceinline__ float sqrt(float x) const
+    {
+        bad |= (__float_as_uint(x) >> 23) - 2u < 250u ? 0u : 1u;  // positive, 2^-125 <= x < 2^125
+        float y;
+        asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+        const float s = x * y;
+        return fmaf(fmaf(-s, s, x), 0.5f * y, s);
+    }
     __device__ __forceinline__ cplx rcp(cplx x) const { return s_rcp(x); }
     __device__ __forceinline__ cplx sqrt(cplx x) const { return s_sqrt(x); }
 };

@@ -243,9 +243,9 @@ template <class S> struct Rec
 // pressure, and the sound speed when asked) are recovered in FP64 before rounding to
 // FP32, so that pressures near vacuum keep their sign; fluxes, Riemann solves and
 // derivatives then run in FP32.  Returns whether it took that path.
-template <int GAS, class S>
+template <int GAS, class S, class M = MathChecked>
 __device__ __forceinline__ bool node_state_f64(const Fr2dArgs& a, const GasParams& g, int64_t off, S s[4],
-                                               NodePrim<S>& pr, S* c)
+                                               NodePrim<S>& pr, S* c, const M& m = M{})
 {
     if constexpr (sizeof(S) == 4)
     {
@@ -253,7 +253,7 @@ __device__ __forceinline__ bool node_state_f64(const Fr2dArgs& a, const GasParam
         {
             double d[4];
             NodeLoader<double>::load(a, off, d);
-            const NodePrim<double> q = node_prim<GAS>(g, d[0], d[1], d[2], d[3]);
+            const NodePrim<double> q = node_prim<GAS>(g, d[0], d[1], d[2], d[3], m);
 #pragma unroll
             for (int i = 0; i < 4; ++i) s[i] = static_cast<float>(d[i]);
             pr.rho_w = static_cast<float>(q.rho_w);
@@ -263,7 +263,7 @@ __device__ __forceinline__ bool node_state_f64(const Fr2dArgs& a, const GasParam
             pr.e = static_cast<float>(q.e);
             pr.p = static_cast<float>(q.p);
             pr.inv_covol = static_cast<float>(q.inv_covol);
-            if (c) *c = static_cast<float>(node_sound_speed<GAS>(g, q));
+            if (c) *c = static_cast<float>(node_sound_speed<GAS>(g, q, m));
             return true;
         }
     }
@@ -709,7 +709,7 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
             const bool bnode = k == 0 || k == N - 1 || l == 0 || l == N - 1;
             S s[4], c = S(0.0);
             NodePrim<S> pr;
-            const bool f64 = node_state_f64<GAS>(a, g, off, s, pr, bnode ? &c : nullptr);
+            const bool f64 = node_state_f64<GAS>(a, g, off, s, pr, bnode ? &c : nullptr, m);
             if (!f64) NodeLoader<S>::load(a, off, s);
             if constexpr (T::JVP)
             {
@@ -747,7 +747,7 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
     auto halo_pass = [&](const auto& m) {
         NodePrim<S> pr;
         S c = S(0.0);
-        const bool f64 = node_state_f64<GAS>(a, g, hoff, hs, pr, &c);
+        const bool f64 = node_state_f64<GAS>(a, g, hoff, hs, pr, &c, m);
         if (!f64)
         {
             pr = node_prim<GAS>(g, hs[0], hs[1], hs[2], hs[3], m);
