@@ -193,7 +193,18 @@ __device__ __forceinline__ NodePrim<S> node_prim(const GasParams& g, S r0, S r1,
 {
     NodePrim<S> q;
     q.rho_w   = s_wrap_positive(r0);
-    q.inv_rho = m.rcp(q.rho_w);
+    if constexpr (GAS == FRSDG_GAS_IDEAL)
+        q.inv_rho = m.rcp(q.rho_w);
+    else
+    {
+        // 1/rho and 1/(1 - b rho) from one reciprocal of their product (a few ulps from
+        // the two quotients; 2 % of the 1024^2 p = 5 residual's time).  At the gas law's
+        // pole rho = 1/b this gives NaN where the quotients give an infinite pressure.
+        const S covol = pfma(cs<S>(-g.b), q.rho_w, cs<S>(1.0));
+        const S both = m.rcp(pmul(q.rho_w, covol));
+        q.inv_rho = pmul(both, covol);
+        q.inv_covol = pmul(both, q.rho_w);
+    }
     q.u       = pmul(r1, q.inv_rho);
     q.v       = pmul(r2, q.inv_rho);
     const S E = s_wrap_positive(r3);
@@ -208,7 +219,6 @@ __device__ __forceinline__ NodePrim<S> node_prim(const GasParams& g, S r0, S r1,
     else
     {
         // p = (gamma - 1) rho (e + a rho) / (1 - b rho) - a rho^2
-        q.inv_covol = m.rcp(pfma(cs<S>(-g.b), q.rho_w, cs<S>(1.0)));
         const S cvT = pfma(cs<S>(g.a), q.rho_w, q.e);
         q.p = pfma(pmul(pmul(gm1, q.rho_w), cvT), q.inv_covol, -pmul(pmul(cs<S>(g.a), q.rho_w), q.rho_w));
     }
