@@ -1248,7 +1248,7 @@ __device__ __forceinline__ void batch_stage_args(Fr2dArgs& a, const BatchInst2D&
 // (instance in group, bx, by), copy the instance's launch arguments (all but the
 // operators, which are the group's) into shared memory and run the residual tile with
 // the stage epilogue.  Inactive instances (clock) are skipped.
-template <class S, int N, int GAS, int RIEM, int VAR>
+template <class S, int N, int GAS, int RIEM, int VAR, bool POST>
 __global__ void __launch_bounds__((Tile2D<S, N, GEO_AFFINE, VAR>::BT)) __maxnreg__((Tile2D<S, N, GEO_AFFINE, VAR>::MAXREG))
 fr2d_batch_kernel(const __grid_constant__ Fr2dBatchArgs b)
 {
@@ -1268,30 +1268,40 @@ fr2d_batch_kernel(const __grid_constant__ Fr2dBatchArgs b)
         __syncthreads();
         if (threadIdx.x == 0) batch_stage_args(sa, in, ck, b.stage, b.mixed != 0);
         __syncthreads();
-        fr2d_tile<S, N, GAS, RIEM, GEO_AFFINE, VAR, true>(sa, b.ops, tm.y, tm.z, smem_raw);
+        fr2d_tile<S, N, GAS, RIEM, GEO_AFFINE, VAR, POST>(sa, b.ops, tm.y, tm.z, smem_raw);
     }
 }
 
-template <class S, int N, int GAS, int RIEM, int VAR>
-cudaError_t launch_fr2d_batch_kernel(const Fr2dBatchArgs& b, int grid, cudaStream_t st, int* occupancy)
+// POST: the instantiation with the stage epilogue, for the stage that carries a post-step
+// (the last); the others skip the epilogue's registers and spills.
+template <class S, int N, int GAS, int RIEM, int VAR, bool POST>
+cudaError_t launch_fr2d_batch_kernel_v(const Fr2dBatchArgs& b, int grid, cudaStream_t st, int* occupancy)
 {
     using T = Tile2D<S, N, GEO_AFFINE, VAR>;
-    auto kern = fr2d_batch_kernel<S, N, GAS, RIEM, VAR>;
+    auto kern = fr2d_batch_kernel<S, N, GAS, RIEM, VAR, POST>;
+    constexpr size_t bytes = POST ? T::bytes_post : T::bytes_launch;
     static bool attr_done[64] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64 || !attr_done[dev])
     {
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(T::bytes_post));
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
         if (e != cudaSuccess) return e;
         e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) attr_done[dev] = true;
     }
-    if (occupancy) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, kern, T::BT, T::bytes_post);
-    if (grid > 0 && b.ntiles > 0) kern<<<grid, T::BT, T::bytes_post, st>>>(b);
+    if (occupancy) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, kern, T::BT, bytes);
+    if (grid > 0 && b.ntiles > 0) kern<<<grid, T::BT, bytes, st>>>(b);
     return cudaGetLastError();
+}
+
+template <class S, int N, int GAS, int RIEM, int VAR>
+cudaError_t launch_fr2d_batch_kernel(const Fr2dBatchArgs& b, int grid, cudaStream_t st, int* occupancy)
+{
+    if (b.stage == 2) return launch_fr2d_batch_kernel_v<S, N, GAS, RIEM, VAR, true>(b, grid, st, occupancy);
+    return launch_fr2d_batch_kernel_v<S, N, GAS, RIEM, VAR, false>(b, grid, st, occupancy);
 }
 
 // Batched stage launcher of one order N (affine geometry): grid CTAs, or with
