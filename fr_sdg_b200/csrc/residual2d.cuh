@@ -69,7 +69,10 @@ __host__ __device__ constexpr int reg_cap(int n, int words, bool f32, int bt)
     // 0.89 -> 0.84 ms); at n = 5 the same cap is faster on the 1024^2 mesh (0.79 -> 0.69
     // ms) but slower on the 64^2 curved vortex of the mixed-precision runs (0.18 -> 0.24 s
     // to t = 10), so n = 5 keeps 80.  FP64: 80 registers, no spills.
-    if (face_tiles(n, words, f32)) return f32 && n == 6 ? 56 : 80;
+#ifndef FRSDG_F32_REG6
+#define FRSDG_F32_REG6 56
+#endif
+    if (face_tiles(n, words, f32)) return f32 && n == 6 ? FRSDG_F32_REG6 : 80;
     // three co-resident CTAs (one for complex): per sub-partition ceil(ctas*warps/4) warps
     return (16384 / (32 * (((words == 2 ? 1 : 3) * (bt / 32) + 3) / 4))) / 8 * 8;
 #endif

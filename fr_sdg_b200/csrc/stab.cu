@@ -261,10 +261,27 @@ template <int N> __device__ __forceinline__ void stab2d_tile(const StabArgs& a, 
                 // ShockSensor::detect_shock (filter.hpp:654-678)
                 // divisions as reciprocals and products (within a few ulps of the
                 // reference's quotients; the 1/gamma_k are shared by every line)
-                double cg0 = a.gam[0] * s_rcp((1.0e-6 + b0) * (1.0e-6 + b0));
-                double cg1 = a.gam[1] * s_rcp((1.0e-6 + b1) * (1.0e-6 + b1));
-                double cg2 = a.gam[2] * s_rcp((1.0e-6 + b2) * (1.0e-6 + b2));
-                const double iws = s_rcp(cg0 + cg1 + cg2);
+                // (the reciprocals' range checks deferred: one branch per group instead of
+                // one per reciprocal, redone with the checked ones when an input left the
+                // fast range; the same results)
+                const double x0 = (1.0e-6 + b0) * (1.0e-6 + b0), x1 = (1.0e-6 + b1) * (1.0e-6 + b1),
+                             x2 = (1.0e-6 + b2) * (1.0e-6 + b2);
+                unsigned bad = 0;
+                const MathDeferred md{bad};
+                double q0 = md.rcp(x0), q1 = md.rcp(x1), q2 = md.rcp(x2);
+                if (bad)
+                {
+                    q0 = s_rcp(x0);
+                    q1 = s_rcp(x1);
+                    q2 = s_rcp(x2);
+                }
+                double cg0 = a.gam[0] * q0;
+                double cg1 = a.gam[1] * q1;
+                double cg2 = a.gam[2] * q2;
+                const double sw = cg0 + cg1 + cg2;
+                unsigned bad_w = 0;
+                double iws = MathDeferred{bad_w}.rcp(sw);
+                if (bad_w) iws = s_rcp(sw);
                 cg0 *= iws;
                 cg1 *= iws;
                 cg2 *= iws;
