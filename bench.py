@@ -437,8 +437,8 @@ def run_ours(args, ws, rank, local):
                  "speedup_vs_fp64": (elapsed_ms / args.steps) / mms,
                  "fp64_stage_ms": sms, "mixed_stage_ms": xms, "mixed_stage_speedup": sms / xms}
         # the FP32 residual with its derivative contractions on the tensor cores (tcgen05,
-        # split TF32, cfg.mixed_tc = 1; p = 4 and 5 only)
-        if wl.cfg.poly_deg in (4, 5):
+        # split TF32, cfg.mixed_tc = 1; p = 4 to 7)
+        if 4 <= wl.cfg.poly_deg <= 7:
             saved_tc = wl.cfg.mixed_tc
             wl.cfg.mixed_tc = 1
             with FRSolver(wl.cfg) as ts:

@@ -574,7 +574,7 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
     constexpr int TX = T::TX, TY = T::TY, NN = T::NN, TE = T::TE, BT = T::BT, NREC = T::NREC;
     using R_t = typename scalar_traits<S>::real;
     constexpr int ND = 4 * NN;
-    static_assert(!TC || (T::F32 && (N == 5 || N == 6)), "tensor-core contractions: FP32 face tiles at n = 5, 6");
+    static_assert(!TC || (T::F32 && N >= 5 && N <= 8), "tensor-core contractions: FP32 at n = 5..8");
     static_assert(!TC || (T::LINES <= BT && BT <= 2 * tc::kTileLines), "one line of each set per thread");
     // every CTA of every mix of these kernels that fits on an SM (228 KB of shared memory)
     // finds its TMEM columns free: columns per byte of shared memory stay below 512 / 228 KB
@@ -1175,9 +1175,9 @@ cudaError_t launch_fr2d_kernel_v(const Fr2dArgs& a, cudaStream_t st)
 template <class S, int N, int GAS, int RIEM, int GEO>
 cudaError_t launch_fr2d_kernel(const Fr2dArgs& a, cudaStream_t st)
 {
-    if constexpr (sizeof(S) == 4 && (N == 5 || N == 6))
+    if constexpr (sizeof(S) == 4 && N >= 5 && N <= 8)
     {
-        // the FP32 face tiles with their derivative contractions on the tensor cores
+        // the FP32 tiles with their derivative contractions on the tensor cores
         if (a.tc && a.mode != MODE_JAC)
         {
             if (a.mode == MODE_STAGE && a.post) return launch_fr2d_kernel_v<S, N, GAS, RIEM, GEO, true, true>(a, st);

@@ -137,7 +137,7 @@ typedef struct frsdg_config {
      * p_bar).  Default 0 (off), pp_eps 1e-13. */
     int32_t pp_limit;
     /* FP32 residual of the mixed form (frsdg_residual_f32, frsdg_rk_stage_mixed, the
-     * FRSDG_STAGE_MIXED stages) at p = 4 and 5 (no counterpart in the reference): 1 = its
+     * FRSDG_STAGE_MIXED stages) at p = 4 to 7 (no counterpart in the reference): 1 = its
      * derivative contractions run on the tensor cores (tcgen05, operands split into
      * TF32 high and low parts, FP32 accumulation), 0 = FP32 FMAs on the CUDA cores.
      * Other orders, FP64 and complex residuals and batch launches ignore it. */

@@ -114,7 +114,7 @@ def test_mixed_vortex_matches_fp64_accuracy(ne, cuda):
 
 
 # ---- the FP32 residual with its derivative contractions on the tensor cores --------
-# (cfg.mixed_tc = 1, p = 4 and 5).  Meshes whose sizes leave partial tiles on both axes.
+# (cfg.mixed_tc = 1, p = 4 to 7).  Meshes whose sizes leave partial tiles on both axes.
 TC_CASES = {
     "cart_vdw_hllc_p4_walls": dict(p=4, n_elems=(9, 5), box=(1.3, 0.9), riemann="hllc", gas="vdw",
                                    vdw=(0.05, 0.02),
@@ -126,6 +126,12 @@ TC_CASES = {
                                          geometry=A.GEOM_SINE_WARP, geom_params=(0.1, 0, 0, 0),
                                          bcs={A.LEFT: PER, A.RIGHT: PER, A.TOP: PER, A.BOTTOM: PER}),
     "bump_hllc_p5_inflow_outlet": dict(CASES["bump_hllc_p3_inflow_outlet"], p=5, n_elems=(11, 3)),
+    "cart_vdw_hllc_p6_walls": dict(p=6, n_elems=(5, 3), box=(1.3, 0.9), riemann="hllc", gas="vdw",
+                                   vdw=(0.05, 0.02),
+                                   bcs={A.LEFT: OUT, A.RIGHT: A.BC_WALL, A.TOP: A.BC_WALL, A.BOTTOM: OUT}),
+    "sinewarp_hllc_p7_periodic": dict(p=7, n_elems=(3, 5), box=(10.0, 10.0), riemann="hllc",
+                                      geometry=A.GEOM_SINE_WARP, geom_params=(0.1, 0, 0, 0),
+                                      bcs={A.LEFT: PER, A.RIGHT: PER, A.TOP: PER, A.BOTTOM: PER}),
 }
 
 
