@@ -1113,7 +1113,7 @@ int frsdg_check_state(frsdg_handle* h, const double* U, void* stream)
 
 int frsdg_device_math(int32_t op, const double* x, double* y, int64_t n, void* stream)
 {
-    if ((op != 0 && op != 1) || n < 0 || (n > 0 && (!x || !y))) return fail(FRSDG_ERR_ARG, "bad argument");
+    if (op < 0 || op > 5 || n < 0 || (n > 0 && (!x || !y))) return fail(FRSDG_ERR_ARG, "bad argument");
     const cudaError_t e = launch_device_math(op, x, y, n, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_fail(e, "device-math launch");
     return FRSDG_OK;

@@ -152,12 +152,43 @@ __global__ void __launch_bounds__(256) check_density_kernel(const double* U, int
 }
 
 // The library's device reciprocal and square root (device_math.cuh), elementwise, for
-// validation against IEEE division and sqrt.
+// validation against IEEE division and sqrt: op 0 / 1 the checked FP64 functions;
+// 2 / 3 the deferred form the residual's node and face passes use (fast path, redone
+// with the checked function when the input left the fast range); 4 / 5 the FP32 fast
+// forms of the mixed residual (MathDeferred on float, redone with the IEEE operations),
+// on x rounded to float, the result widened to double.
 __global__ void device_math_kernel(int op, const double* x, double* y, int64_t n)
 {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    y[i] = op == 0 ? s_rcp(x[i]) : s_sqrt(x[i]);
+    const double v = x[i];
+    unsigned bad = 0;
+    const MathDeferred md{bad};
+    double r;
+    switch (op)
+    {
+        case 0: r = s_rcp(v); break;
+        case 1: r = s_sqrt(v); break;
+        case 2: r = md.rcp(v); if (bad) r = s_rcp(v); break;
+        case 3: r = md.sqrt(v); if (bad) r = s_sqrt(v); break;
+        case 4:
+        {
+            const float f = static_cast<float>(v);
+            float q = md.rcp(f);
+            if (bad) q = s_rcp(f);
+            r = q;
+            break;
+        }
+        default:
+        {
+            const float f = static_cast<float>(v);
+            float q = md.sqrt(f);
+            if (bad) q = s_sqrt(f);
+            r = q;
+            break;
+        }
+    }
+    y[i] = r;
 }
 
 } // namespace

@@ -390,7 +390,11 @@ int frsdg_check_state(frsdg_handle* h, const double* U, void* stream);
 /* The library's device FP64 reciprocal (op 0) and square root (op 1) -- a
  * single-precision seed refined by Newton steps, used throughout the residual --
  * applied elementwise to the device array x[0..n) into y, for validation against
- * IEEE division and sqrt.  No handle needed. */
+ * IEEE division and sqrt.  Ops 2 and 3: the same in the deferred form of the residual's
+ * node and face passes (the fast path, redone with ops 0 / 1 when the input lies
+ * outside its range; equal to ops 0 / 1).  Ops 4 and 5: the FP32 reciprocal and square
+ * root of the FP32 residual, on x rounded to float (results widened to double).  No
+ * handle needed. */
 int frsdg_device_math(int32_t op, const double* x, double* y, int64_t n, void* stream);
 
 /* The split-precision tensor-core contraction of the FP32 residual on its own, for

@@ -3,6 +3,8 @@ the nodes a host-injected state poisons (NaN or non-positive density), frsdg_che
 covers states no residual has read, the integrator rejects and retakes failed steps
 with halved dt -- and the library's FP64 reciprocal and square root against IEEE
 division and sqrt."""
+import math
+
 import numpy as np
 import pytest
 import torch
@@ -92,14 +94,52 @@ def test_device_reciprocal_and_sqrt_within_two_ulp(op, cuda):
         x = torch.where(torch.rand(1_000_000, generator=g) < 0.5, x, -x)
     edge = torch.tensor([1.0, 2.0, 0.5, 3.0, 1e-37, 1e37, 1.1e-37, 0.9e37, 1e-300, 1e300, 2.2250738585072014e-308,
                          4.9e-324, 1e-310, 1.7976931348623157e308, 0.0, -0.0, float("inf"), -float("inf"),
-                         float("nan"), -1.0, -1e-200], dtype=torch.float64)
+                         float("nan"), -1.0, -1e-200,
+                         # the edges of the fast paths' range [2^-122, 2^123)
+                         2.0 ** -122, math.nextafter(2.0 ** -122, 0.0), 2.0 ** 123, math.nextafter(2.0 ** 123, 0.0),
+                         -2.0 ** -122, -math.nextafter(2.0 ** 123, 0.0)], dtype=torch.float64)
     x = torch.cat([x, edge]).to(cuda)
     y = torch.empty_like(x)
     A.check(A.lib().frsdg_device_math(0 if op == "rcp" else 1, x.data_ptr(), y.data_ptr(), x.numel(), None),
             "frsdg_device_math")
+    # the deferred form of the residual's passes equals the checked function bit for bit
+    yd = torch.empty_like(x)
+    A.check(A.lib().frsdg_device_math(2 if op == "rcp" else 3, x.data_ptr(), yd.data_ptr(), x.numel(), None),
+            "frsdg_device_math")
     torch.cuda.synchronize()
+    assert torch.equal(torch.isnan(yd), torch.isnan(y))
+    assert torch.equal(yd[~torch.isnan(y)], y[~torch.isnan(y)])
     ref = 1.0 / x if op == "rcp" else torch.sqrt(x)
     fin = torch.isfinite(ref) & (ref != 0)
     assert torch.equal(torch.isnan(y), torch.isnan(ref))
     assert torch.equal(y[~fin & ~torch.isnan(ref)], ref[~fin & ~torch.isnan(ref)])  # +-inf and +-0 alike
     assert int(_ulps(y[fin], ref[fin]).max()) <= 2
+
+
+@pytest.mark.parametrize("op", ["rcp", "sqrt"])
+def test_fp32_fast_reciprocal_and_sqrt_within_two_ulp(op, cuda):
+    """The FP32 reciprocal and square root of the mixed residual (hardware approximation
+    plus one Newton step, IEEE operations outside [2^-125, 2^125)) against IEEE float
+    division and sqrt: within 2 float ulps, zeros, infinities and NaNs alike."""
+    g = torch.Generator(device="cpu").manual_seed(25)
+    exps = torch.randint(-140, 128, (1_000_000,), generator=g).to(torch.float64)
+    mant = 1.0 + torch.rand(1_000_000, generator=g, dtype=torch.float64)
+    xf = (mant * torch.pow(2.0, exps)).float()
+    if op == "rcp":
+        xf = torch.where(torch.rand(1_000_000, generator=g) < 0.5, xf, -xf)
+    edge = torch.tensor([1.0, 2.0, 0.5, 3.0, 2.0 ** -125, 2.0 ** 125, 2.0 ** 124, 1e-45, 1e-40, 3.4e38, 0.0, -0.0,
+                         float("inf"), -float("inf"), float("nan"), -1.0], dtype=torch.float32)
+    xf = torch.cat([xf, edge])
+    x = xf.double().to(cuda)
+    y = torch.empty_like(x)
+    A.check(A.lib().frsdg_device_math(4 if op == "rcp" else 5, x.data_ptr(), y.data_ptr(), x.numel(), None),
+            "frsdg_device_math")
+    torch.cuda.synchronize()
+    got = y.float().cpu()
+    ref = 1.0 / xf if op == "rcp" else torch.sqrt(xf)
+    assert torch.equal(torch.isnan(got), torch.isnan(ref))
+    fin = torch.isfinite(ref) & (ref != 0) & (ref.abs() >= torch.finfo(torch.float32).tiny)
+    other = ~fin & ~torch.isnan(ref)
+    assert torch.equal(got[other & ((ref == 0) | torch.isinf(ref))], ref[other & ((ref == 0) | torch.isinf(ref))])
+    ulps = (got[fin].view(torch.int32).long() - ref[fin].view(torch.int32).long()).abs()
+    assert int(ulps.max()) <= 2
