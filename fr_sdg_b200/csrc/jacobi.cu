@@ -271,11 +271,10 @@ cudaError_t launch_block_gs(const float* inv, const float* off, const double* r,
 {
     if (n % 4 != 0 || n / 4 > kGsThreads) return cudaErrorInvalidValue;
     const int tpe = n / 4, epc = kGsThreads / tpe;
-    const size_t smem = size_t(epc) * 5 * n * sizeof(double);
-    const int64_t slots = int64_t((Nx + 1) / 2) * Ny;  // element slots of one colour
+    const size_t smem = size_t(epc) * 5 * n * sizeof(double);  // at most 20.5 KB for n <= 144
+    const int64_t slots = int64_t((Nx + 1) / 2) * Ny;            // element slots of one colour
     const unsigned grid = unsigned((slots + epc - 1) / epc);
-    cudaError_t e = cudaFuncSetAttribute(block_gs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
+    cudaError_t e;
     for (int phase = 0; phase < 3; ++phase)
     {
         block_gs_kernel<<<grid, kGsThreads, smem, s>>>(inv, off, r, z, n, Nx, Ny, phase, epc);

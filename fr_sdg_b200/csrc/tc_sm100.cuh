@@ -146,7 +146,8 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Poll the barrier for the phase with parity `parity`; false after `limit` polls.
+// Poll the barrier for the phase with parity `parity` (non-blocking test, a 64 ns sleep
+// between polls); false after `limit` polls, i.e. after at least limit x 64 ns.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit)
 {
     const uint32_t a = smem_u32(bar);
@@ -155,12 +156,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int li
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t}"
             : "=r"(done)
             : "r"(a), "r"(parity)
             : "memory");
         if (done) return true;
+        __nanosleep(64);
     }
     return false;
 }
