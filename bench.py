@@ -30,7 +30,8 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "DOF-residuals/s (FP64 FR residual, rhs_func)"
 UNIT = "DOF-residuals/s"
-WORKLOAD = "blast_vdw_1024x1024_p5 (2D radial blast, HLLC, Van der Waals a=0.05 b=0.02, WENO + shock sensor)"
+WORKLOAD = ("blast_vdw_1024x1024_p5 (2D radial blast, HLLC, Van der Waals a=0.05 b=0.02, spectral filter with "
+            "the shock sensor)")
 
 
 def dist_env():
