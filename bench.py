@@ -520,6 +520,29 @@ def run_ours(args, ws, rank, local):
         e2e = {"value": ws * dofs * ke / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": Uh.numel() * 8,
                "d2h_bytes_per_step": Fh.numel() * 8, "steps": ke,
                "path": "frsdg_rhs_host (pinned host U -> device -> rhs -> pinned host)"}
+        # the bound of this path: the same bytes copied both ways at once, pinned host
+        # memory, no compute (the residual hides behind the transfers when the step
+        # takes as long as the copies alone)
+        dU, dF = torch.empty_like(U), torch.empty_like(U)
+        cs1, cs2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+        def copies():
+            with torch.cuda.stream(cs1):
+                dU.copy_(Uh, non_blocking=True)
+            with torch.cuda.stream(cs2):
+                Fh.copy_(dF, non_blocking=True)
+
+        copies()
+        torch.cuda.synchronize()
+        c0 = time.perf_counter()
+        for _ in range(ke):
+            copies()
+        torch.cuda.synchronize()
+        cms = (time.perf_counter() - c0) * 1e3 / ke
+        e2e["copy_bound"] = {"ms_per_step": cms, "gb_per_s_both_directions": 2 * Uh.numel() * 8 / cms / 1e6,
+                             "value": ws * dofs / (cms / 1e3), "frac": (ws * dofs * ke / (ems / 1e3)) /
+                             (ws * dofs / (cms / 1e3))}
+        del dU, dF
 
     # ---- roofline of the residual kernel
     peak, peak_kind = measured_peaks()
