@@ -724,7 +724,12 @@ __device__ __forceinline__ void fr2d_tile(const Fr2dArgs& a, const Ops& ops, int
             if (!f64)
             {
                 pr = node_prim<GAS>(g, s[0], s[1], s[2], s[3], m);
-                c = node_sound_speed<GAS>(g, pr, m);
+                if constexpr (T::JVP)
+                {
+                    if (bnode) c = node_sound_speed<GAS>(g, pr, m);  // a complex square root
+                }
+                else
+                    c = node_sound_speed<GAS>(g, pr, m);
             }
             const S rEp = s[3] + pr.p;
             const S ruv = s[1] * pr.v;
