@@ -68,13 +68,14 @@ template <class PA> __device__ __forceinline__ double node_wave_speed(const PA& 
 // The same quantities with reciprocals (device_math.cuh: within 2 ulp of the
 // quotients): the screen that lets admissible elements skip the limiter, and the wave
 // speed of the adaptive time step, where rounding is immaterial.
-template <class PA> __device__ __forceinline__ double pp_pressure_fast(const PA& a, const double* u)
+template <class PA, class M = MathChecked>
+__device__ __forceinline__ double pp_pressure_fast(const PA& a, const double* u, const M& m = M{})
 {
-    const double ir = s_rcp(u[0]);
+    const double ir = m.rcp(u[0]);
     const double rho_e = u[3] - 0.5 * (u[1] * u[1] + u[2] * u[2]) * ir;  // rho e
     if (a.gas_law == FRSDG_GAS_IDEAL) return (a.gas.gamma - 1.0) * rho_e;
     const double rho = u[0];
-    return ((a.gas.gamma - 1.0) * (rho_e + a.gas.a * rho * rho)) * s_rcp(1.0 - a.gas.b * rho) - a.gas.a * rho * rho;
+    return ((a.gas.gamma - 1.0) * (rho_e + a.gas.a * rho * rho)) * m.rcp(1.0 - a.gas.b * rho) - a.gas.a * rho * rho;
 }
 template <class PA> __device__ __forceinline__ double node_wave_speed_fast(const PA& a, const double* u)
 {
@@ -135,7 +136,11 @@ __device__ __forceinline__ void pp_element2d(const PA& a, double* base, float* b
     // screen: an element whose nodes all have density and pressure above eps0 is left
     // as it is (eps <= eps0), so it needs no cell average (nodes within 1e-10 of the
     // floor take the exact path)
+    // (the pressures' reciprocals with deferred range checks: one redo of the screen when
+    // an input left the fast range, instead of a branch per reciprocal; the same result)
     bool clear = true;
+    unsigned bad = 0;
+    const double thr = a.eps0 * (1.0 + 1e-10);
 #pragma unroll
     for (int r = 0; r < R; ++r)
     {
@@ -146,9 +151,15 @@ __device__ __forceinline__ void pp_element2d(const PA& a, double* base, float* b
             const double2 x0 = *reinterpret_cast<const double2*>(base + q * 4);
             const double2 x1 = *reinterpret_cast<const double2*>(base + q * 4 + 2);
             u[r][0] = x0.x; u[r][1] = x0.y; u[r][2] = x1.x; u[r][3] = x1.y;
-            const double thr = a.eps0 * (1.0 + 1e-10);
-            clear = clear && u[r][0] > thr && pp_pressure_fast(a, u[r]) > thr;
+            clear = clear && u[r][0] > thr && pp_pressure_fast(a, u[r], MathDeferred{bad}) > thr;
         }
+    }
+    if (bad)
+    {
+        clear = true;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (lane + 32 * r < NQ) clear = clear && u[r][0] > thr && pp_pressure_fast(a, u[r]) > thr;
     }
     if (__all_sync(0xffffffffu, clear || !limit))
     {

@@ -509,8 +509,18 @@ __device__ __forceinline__ void stage_epilogue(const Fr2dArgs& a, const Ops& ops
             const double2 x0 = *reinterpret_cast<const double2*>(sX + q * 4);
             const double2 x1 = *reinterpret_cast<const double2*>(sX + q * 4 + 2);
             const double u[4] = {x0.x, x0.y, x1.x, x1.y};
-            if (limit && !(u[0] > thr && pp_pressure_fast(v, u) > thr)) s_flag[e] = 1;
-            else if (want_amax) w = fmax(w, node_wave_speed_fast(v, u));
+            if (limit)
+            {
+                unsigned bad = 0;
+                double p = pp_pressure_fast(v, u, MathDeferred{bad});
+                if (bad) p = pp_pressure_fast(v, u);
+                if (!(u[0] > thr && p > thr))
+                {
+                    s_flag[e] = 1;
+                    continue;
+                }
+            }
+            if (want_amax) w = fmax(w, node_wave_speed_fast(v, u));
         }
         if (want_amax)
         {
